@@ -1,0 +1,208 @@
+/* snogray_b200.h -- C ABI of the B200 path-tracing backend.
+ *
+ * This is the drop-in boundary for snogray's render path: plain C types,
+ * host or device pointers with sizes, opaque handles, int status codes.  A
+ * host program (the reference-shaped C++ classes in snogray_b200.hpp, the
+ * Python package snogray_b200, or a binding generated from this header)
+ * describes a scene once, then renders it or traces ray batches through it.
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * relative to the snogray source tree).
+ *
+ * Errors: every function returns SNOG_OK (0) or a positive SNOG_E* code and
+ * never throws or aborts; snog_last_error() gives a message for the calling
+ * thread's most recent failure.  The reference reports the same conditions
+ * with std::runtime_error (render/global-render-state.cc:73-74,90,
+ * light/surface-light-sampler.cc:30-36).
+ *
+ * Threading: functions taking a SnogScene may be called from several threads
+ * for different scenes; calls on one scene are serialised by the library.
+ */
+#ifndef SNOGRAY_B200_H
+#define SNOGRAY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum SnogStatus {
+  SNOG_OK = 0,
+  SNOG_EINVAL = 1,      /* bad argument or scene description */
+  SNOG_ENOMEM = 2,      /* device or host allocation failed / over budget */
+  SNOG_ECUDA = 3,       /* CUDA runtime error */
+  SNOG_ETIMEOUT = 4,    /* a bounded device wait ran out */
+  SNOG_EBUSY = 5,       /* result not ready yet */
+  SNOG_ENOTFOUND = 6,   /* unknown handle / job id */
+  SNOG_ECANCELED = 7    /* job was cancelled */
+};
+
+/* Material kinds; the records mirror the reference constructors. */
+enum SnogMaterialType {
+  SNOG_LAMBERT = 0,        /* Lambert (color)                  material/lambert.h */
+  SNOG_COOK_TORRANCE = 1,  /* CookTorrance (color, gloss, m, Ior) material/cook-torrance.h:27-30 */
+  SNOG_MIRROR = 2,         /* Mirror (Ior, reflectance, color) material/mirror.h:47-49 */
+  SNOG_GLASS = 3,          /* Glass (Medium (ior, absorb))     material/glass.h:27 */
+  SNOG_GLOW = 4            /* Glow (color [, underlying])      material/glow.h:28-30 */
+};
+
+typedef struct SnogMaterial {
+  uint32_t type;
+  float color[3];      /* Lambert colour, CT diffuse, Mirror underlying, Glow emission */
+  float gloss[3];      /* CT gloss colour, Mirror reflectance */
+  float m;             /* CT rms microfacet slope */
+  float ior_n, ior_k;  /* CT/Mirror Ior (n + ik); Glass medium ior (n) */
+  float absorb[3];     /* Glass medium absorption */
+  int32_t underlying;  /* Glow: index of an earlier material, or -1 */
+} SnogMaterial;
+
+typedef struct SnogSphere { float center[3]; float radius; uint32_t material; } SnogSphere;
+
+/* Tripar (surface/tripar.h): corner v0, edges e1, e2; normal = e2 x e1. */
+typedef struct SnogTripar {
+  float v0[3], e1[3], e2[3];
+  uint32_t parallelogram;
+  uint32_t material;
+} SnogTripar;
+
+/* PointLight (light/point-light.h:32-47); angle >= 2*pi means omni. */
+typedef struct SnogPointLight {
+  float pos[3]; float color[3]; float angle; float fringe_angle; float dir[3];
+} SnogPointLight;
+
+/* FarLight (light/far-light.h:39-45). */
+typedef struct SnogFarLight { float dir[3]; float angle; float color[3]; } SnogFarLight;
+
+/* A scene, as the reference's SurfaceGroup holds it: one triangle mesh whose
+ * parts are runs of equal tri_material (non-decreasing), spheres, tripars,
+ * explicit lights and at most one lat-long envmap light (light/envmap-light.h,
+ * texture/spheremap.h).  Surfaces whose material is a Glow become area
+ * lights, as Primitive::add_light_samplers does (surface/primitive.cc:48-54).
+ * Primitive ids: triangles [0,nt), spheres [nt,nt+ns), tripars after.
+ * All arrays are host memory, read during snog_scene_create only. */
+typedef struct SnogSceneDesc {
+  uint32_t n_materials; const SnogMaterial *materials;
+  uint32_t n_vertices; const float *vertices;          /* 3 floats each */
+  uint32_t n_triangles; const uint32_t *triangles;     /* 3 indices each */
+  const uint32_t *tri_material;
+  uint32_t n_spheres; const SnogSphere *spheres;
+  uint32_t n_tripars; const SnogTripar *tripars;
+  uint32_t n_point_lights; const SnogPointLight *point_lights;
+  uint32_t n_far_lights; const SnogFarLight *far_lights;
+  uint32_t env_width, env_height;                      /* 0 = none; width = 2*height */
+  const float *env_rgb;                                /* env_height rows of env_width RGB, top row first */
+  float env_frame[9];                                  /* envmap light frame axes x, y, z */
+} SnogSceneDesc;
+
+/* Camera as the reference holds it after move/point/set_fov
+ * (camera/camera.h:84-128, 231-242, 384-389). */
+typedef struct SnogCamera {
+  float pos[3], forward[3], right[3], up[3];
+  float tan_half_fov_x, tan_half_fov_y;
+} SnogCamera;
+
+/* Render parameters: the reference's ValTable keys in brackets. */
+typedef struct SnogRenderParams {
+  uint32_t width, height;
+  uint32_t spp;              /* [samples] */
+  uint32_t min_path_len;     /* [surface_integ.min_path_len], default 3 */
+  uint32_t max_path_len;     /* [surface_integ.max_path_len], default 25 */
+  uint32_t direct_samples;   /* [surface_integ.direct_samples], default 1 */
+  float min_trace;           /* [min_trace], default 1e-3 */
+  float bg_alpha;            /* [background_alpha], default 1 */
+  uint64_t seed;             /* stream selector for the GPU's counter-based RNG */
+} SnogRenderParams;
+
+typedef struct SnogSceneInfo {
+  uint32_t n_nodes, n_plist, max_depth, n_leaf_nodes;
+  uint32_t n_triangles, n_spheres, n_tripars, n_lights;
+  uint64_t n_list_surfaces;       /* surface references in all node lists */
+  float origin[3], size;          /* octree root cube */
+  float bbox_min[3], bbox_max[3];
+  float horizon;
+  uint64_t device_bytes;
+  double build_ms;
+} SnogSceneInfo;
+
+typedef struct SnogRenderStats {
+  uint64_t paths;            /* camera samples traced (pattern incl. filter margin) */
+  uint64_t closest_rays;     /* closest-hit queries (Scene::intersect) */
+  uint64_t shadow_rays;      /* any-hit queries (Scene::occludes) */
+  double device_ms;          /* device time of the render, CUDA events */
+  uint32_t waves;            /* wavefront batches the render was split into */
+  uint32_t kernel_launches;
+} SnogRenderStats;
+
+typedef struct SnogScene SnogScene;
+
+/* Library version string. */
+const char *snog_version(void);
+
+/* Message for the calling thread's last failing call ("" if none). */
+const char *snog_last_error(void);
+
+/* Select the CUDA device used by subsequent calls from this process. */
+int snog_init(int device);
+
+/* Build the acceleration structure and upload the scene.  Replaces
+ * GlobalRenderState (render/global-render-state.cc:28-49) -> Scene
+ * (render/scene.cc:26-44) -> Octree::Builder (space/octree-builder.cc:173-650),
+ * Scene::light_samplers and EnvmapLight::Sampler's Hist2dDist
+ * (light/envmap-light.cc:103-140, geometry/hist-2d-dist.cc:65-120). */
+int snog_scene_create(const SnogSceneDesc *desc, SnogScene **out);
+
+/* Build the acceleration structure on the host only, without touching the
+ * device (no CUDA context needed): the handle serves snog_scene_info and
+ * snog_scene_octree, and is refused by the tracing and rendering calls. */
+int snog_scene_build_host(const SnogSceneDesc *desc, SnogScene **out);
+
+int snog_scene_destroy(SnogScene *scene);
+
+/* Octree statistics and sizes; replaces Octree::stats (space/octree.cc:308-367). */
+int snog_scene_info(const SnogScene *scene, SnogSceneInfo *info);
+
+/* Copy the octree out: children (8*n_nodes), heads (n_nodes), and the packed
+ * surface lists as primitive ids with -1 ending each list (n_plist).  This is
+ * the reference's Octree::nodes / surface_ptrs (space/octree.h:111-121). */
+int snog_scene_octree(const SnogScene *scene, uint32_t *children, uint32_t *heads,
+                      int32_t *plist);
+
+/* Closest-hit / any-hit queries for a ray batch in HOST memory, SoA:
+ * rays = ox[n] oy[n] oz[n] dx[n] dy[n] dz[n] tmax[n], t0 = 0.  Rays [0,
+ * n_closest) are closest-hit queries (Space::intersect, space/space.cc:72-84),
+ * the rest any-hit queries (Space::intersects, space/space.cc:120-129).
+ * prim[i] = id of the hit primitive or -1; for an any-hit query it is the
+ * primitive that stopped the search.  t[i] = hit distance (closest queries),
+ * normal = world-space geometric normal (3 per ray, may be NULL).  Counters
+ * (may be NULL): node visits and primitive tests per query kind, in the
+ * reference's RenderStats::IsecStats sense without the negative cache. */
+int snog_trace(SnogScene *scene, const float *rays, uint32_t n, uint32_t n_closest,
+               int32_t *prim, float *t, float *normal, uint64_t *counters4);
+
+/* The same with DEVICE pointers, asynchronous on STREAM (a cudaStream_t,
+ * NULL = default stream). */
+int snog_trace_device(SnogScene *scene, const float *d_rays, uint32_t n, uint32_t n_closest,
+                      int32_t *d_prim, float *d_t, float *d_normal, void *stream);
+
+/* Render the whole image with the path integrator and the Mitchell-filtered
+ * sampled output, into HOST memory out_rgb (height rows of width RGB floats,
+ * top row first; the flushed values of ImageSampledOutput,
+ * image/image-sampled-output.cc:79-123).  Replaces RenderMgr::render
+ * (render-mgr/render-mgr.cc:50-74) with PathInteg (render/path-integ.cc:134-407).
+ * The rendered pattern includes the filter margin, as snogray.lua:543-550. */
+int snog_render(SnogScene *scene, const SnogCamera *camera, const SnogRenderParams *params,
+                float *out_rgb, SnogRenderStats *stats);
+
+/* The same with a DEVICE output buffer, asynchronous on STREAM; stats (may
+ * be NULL) are filled after an internal synchronisation only if non-NULL. */
+int snog_render_device(SnogScene *scene, const SnogCamera *camera,
+                       const SnogRenderParams *params, float *d_out_rgb, void *stream,
+                       SnogRenderStats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SNOGRAY_B200_H */

@@ -1,0 +1,188 @@
+"""Oracle-side tooling: scene-spec files and the reference harness runner.
+
+TEST INFRASTRUCTURE.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline / reference legs import this module.  It writes the scene-spec and
+ray-batch files read by oracle/ref_harness.cc (the reference renderer driven
+through its own C++ API) and by the restatement in oracle/port.cc, runs those
+programs, and parses their output.  The layout matches oracle/scene_spec.h.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+REFERENCE_TREE = "/root/reference"
+
+
+def ref_binary(flavour="parity"):
+    return os.path.join(REF_DIR, f"snog_ref_{flavour}")
+
+
+def port_binary():
+    return os.path.join(REF_DIR, "snog_port")
+
+
+def have_ref(flavour="parity"):
+    return os.access(ref_binary(flavour), os.X_OK)
+
+
+def build(targets=("all",), quiet=True):
+    """Build the oracle.  The reference flavours need the reference tree,
+    which exists only on the development machine; the restatement builds
+    anywhere with g++."""
+    tg = list(targets)
+    if "all" in tg and not os.path.isdir(REFERENCE_TREE):
+        tg = ["port"]
+    out = subprocess.run(["make", "-C", HERE, "-j8", *tg], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
+    return out
+
+
+def ensure_port():
+    if not os.access(port_binary(), os.X_OK) or not os.path.exists(os.path.join(REF_DIR, "libsnogport.so")):
+        build(["port"])
+    return port_binary()
+
+
+def write_spec(path, scene, camera=None, params=None):
+    """Write SCENE (snogray_b200.scenes.SceneData) with CAMERA and PARAMS."""
+    from snogray_b200.scenes import RenderParams, Camera
+    params = params or RenderParams()
+    camera = camera or Camera()
+    env = scene.envmap
+    env_h, env_w = (env.shape[0], env.shape[1]) if env is not None else (0, 0)
+    hdr = bytearray()
+    hdr += b"SNOGSPC1"
+    hdr += np.array([len(scene.materials), len(scene.vertices), len(scene.triangles),
+                     len(scene.spheres), len(scene.tripars), len(scene.point_lights),
+                     len(scene.far_lights), env_w, env_h], "<u4").tobytes()
+    hdr += np.asarray(scene.env_frame, "<f4").reshape(9).tobytes()
+    for v in (camera.pos, camera.forward, camera.right, camera.up):
+        hdr += np.asarray(v, "<f4").reshape(3).tobytes()
+    hdr += np.array([camera.tan_half_fov_x, camera.tan_half_fov_y], "<f4").tobytes()
+    hdr += np.array([params.width, params.height, params.spp, params.min_path_len,
+                     params.max_path_len, params.direct_samples], "<u4").tobytes()
+    hdr += np.array([params.min_trace, params.bg_alpha], "<f4").tobytes()
+    hdr += np.zeros(8, "<u4").tobytes()
+    with open(path, "wb") as f:
+        f.write(hdr)
+        f.write(np.ascontiguousarray(scene.materials).tobytes())
+        f.write(np.ascontiguousarray(scene.vertices, "<f4").tobytes())
+        f.write(np.ascontiguousarray(scene.triangles, "<u4").tobytes())
+        f.write(np.ascontiguousarray(scene.tri_mat, "<u4").tobytes())
+        f.write(np.ascontiguousarray(scene.spheres).tobytes())
+        f.write(np.ascontiguousarray(scene.tripars).tobytes())
+        f.write(np.ascontiguousarray(scene.point_lights).tobytes())
+        f.write(np.ascontiguousarray(scene.far_lights).tobytes())
+        if env is not None:
+            f.write(np.ascontiguousarray(env, "<f4").tobytes())
+
+
+def write_rays(path, soa, n_closest):
+    soa = np.ascontiguousarray(soa, np.float32)
+    n = soa.shape[1]
+    with open(path, "wb") as f:
+        f.write(np.array([n, n_closest], "<u4").tobytes())
+        f.write(soa.tobytes())
+
+
+def _run(cmd, timeout=3600):
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if out.returncode != 0:
+        raise RuntimeError(f"{cmd[0]} failed ({out.returncode}): {out.stderr[-2000:]}")
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    return json.loads(lines[-1]) if lines else {}
+
+
+def read_octree(path):
+    raw = np.fromfile(path, np.uint8)
+    hdr_f = raw[:16].view("<f4")
+    n_nodes, n_list = raw[16:24].view("<u4")
+    nodes = raw[24:24 + 36 * n_nodes].view("<u4").reshape(n_nodes, 9)
+    lst = raw[24 + 36 * n_nodes:24 + 36 * n_nodes + 4 * n_list].view("<i4")
+    return {"origin": hdr_f[:3].copy(), "size": float(hdr_f[3]), "children": nodes[:, :8].copy(),
+            "heads": nodes[:, 8].copy(), "list": lst.copy()}
+
+
+def read_trace(path, n):
+    raw = np.fromfile(path, np.uint8)
+    prim = raw[:4 * n].view("<i4").copy()
+    t = raw[4 * n:8 * n].view("<f4").copy()
+    nrm = raw[8 * n:20 * n].view("<f4").reshape(n, 3).copy()
+    st = raw[20 * n:20 * n + 80].view("<u8").reshape(2, 5)
+    keys = ["surface_tests", "surface_hits", "neg_cache_hits", "neg_cache_collisions", "node_calls"]
+    return prim, t, nrm, {"closest": dict(zip(keys, map(int, st[0]))),
+                          "any": dict(zip(keys, map(int, st[1])))}
+
+
+def read_pfm(path):
+    with open(path, "rb") as f:
+        kind = f.readline().strip()
+        w, h = map(int, f.readline().split())
+        scale = float(f.readline())
+        data = np.frombuffer(f.read(), "<f4" if scale < 0 else ">f4")
+    ch = 3 if kind == b"PF" else 1
+    img = data.reshape(h, w, ch).astype(np.float32)
+    return img[::-1].copy()     # PFM stores the bottom row first
+
+
+def ref_octree(scene, flavour="parity", tmpdir=None):
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, op = os.path.join(d, "s.spec"), os.path.join(d, "o.bin")
+        write_spec(sp, scene)
+        stats = _run([ref_binary(flavour), "octree", sp, op])
+        oc = read_octree(op)
+    oc["stats"] = stats
+    return oc
+
+
+def ref_trace(scene, soa, n_closest, threads=8, flavour="parity", tmpdir=None):
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, rp, op = (os.path.join(d, x) for x in ("s.spec", "r.bin", "o.bin"))
+        write_spec(sp, scene)
+        write_rays(rp, soa, n_closest)
+        info = _run([ref_binary(flavour), "trace", sp, rp, op, str(threads)])
+        prim, t, nrm, stats = read_trace(op, soa.shape[1])
+    return prim, t, nrm, stats, info
+
+
+def ref_render(scene, camera, params, threads=1, seed_skip=0, spp=0, row0=0, rows=0,
+               flavour="parity", tmpdir=None, timeout=7200):
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, op = os.path.join(d, "s.spec"), os.path.join(d, "o.pfm")
+        write_spec(sp, scene, camera, params)
+        info = _run([ref_binary(flavour), "render", sp, op, str(threads), str(seed_skip),
+                     str(spp), str(row0), str(rows)], timeout=timeout)
+        img = read_pfm(op)
+    return img, info
+
+
+def port_trace(scene, soa, n_closest, threads=8, tmpdir=None):
+    """Closest/any-hit through the restatement (oracle/port.cc)."""
+    exe = ensure_port()
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, rp, op = (os.path.join(d, x) for x in ("s.spec", "r.bin", "o.bin"))
+        write_spec(sp, scene)
+        write_rays(rp, soa, n_closest)
+        info = _run([exe, "trace", sp, rp, op, str(threads)])
+        prim, t, nrm, stats = read_trace(op, soa.shape[1])
+    return prim, t, nrm, stats, info
+
+
+def port_octree(scene, tmpdir=None):
+    exe = ensure_port()
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, op = os.path.join(d, "s.spec"), os.path.join(d, "o.bin")
+        write_spec(sp, scene)
+        stats = _run([exe, "octree", sp, op])
+        oc = read_octree(op)
+    oc["stats"] = stats
+    return oc

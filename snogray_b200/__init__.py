@@ -1,0 +1,268 @@
+"""snogray_b200 -- B200 path-tracing backend for snogray's render path.
+
+Python face of the C ABI in include/snogray_b200.h (loaded with ctypes from
+the in-tree libsnogray_b200.so).  There is no fallback: if the shared library
+is missing or fails to load, importing this package raises.
+
+    from snogray_b200 import Scene, scenes
+    sd = scenes.cornell_box()
+    with Scene(sd) as sc:
+        img, stats = sc.render(scenes.cornell_camera(256, 256), scenes.cornell_params())
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import scenes  # noqa: F401  (re-exported)
+from .scenes import Camera, RenderParams, SceneData
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsnogray_b200.so")
+
+SNOG_OK, SNOG_EINVAL, SNOG_ENOMEM, SNOG_ECUDA, SNOG_ETIMEOUT, SNOG_EBUSY, SNOG_ENOTFOUND, \
+    SNOG_ECANCELED = range(8)
+
+
+class SnogError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"snogray_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m snogray_b200.build`")
+    return C.CDLL(LIB_PATH)
+
+
+_lib = _load()
+
+
+# --- C structs (must match include/snogray_b200.h) -------------------------
+
+class SnogSceneDesc(C.Structure):
+    _fields_ = [("n_materials", C.c_uint32), ("materials", C.c_void_p),
+                ("n_vertices", C.c_uint32), ("vertices", C.c_void_p),
+                ("n_triangles", C.c_uint32), ("triangles", C.c_void_p),
+                ("tri_material", C.c_void_p),
+                ("n_spheres", C.c_uint32), ("spheres", C.c_void_p),
+                ("n_tripars", C.c_uint32), ("tripars", C.c_void_p),
+                ("n_point_lights", C.c_uint32), ("point_lights", C.c_void_p),
+                ("n_far_lights", C.c_uint32), ("far_lights", C.c_void_p),
+                ("env_width", C.c_uint32), ("env_height", C.c_uint32),
+                ("env_rgb", C.c_void_p), ("env_frame", C.c_float * 9)]
+
+
+class SnogCamera(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("forward", C.c_float * 3), ("right", C.c_float * 3),
+                ("up", C.c_float * 3), ("tan_half_fov_x", C.c_float), ("tan_half_fov_y", C.c_float)]
+
+
+class SnogRenderParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("min_path_len", C.c_uint32), ("max_path_len", C.c_uint32),
+                ("direct_samples", C.c_uint32), ("min_trace", C.c_float), ("bg_alpha", C.c_float),
+                ("seed", C.c_uint64)]
+
+
+class SnogSceneInfo(C.Structure):
+    _fields_ = [("n_nodes", C.c_uint32), ("n_plist", C.c_uint32), ("max_depth", C.c_uint32),
+                ("n_leaf_nodes", C.c_uint32), ("n_triangles", C.c_uint32),
+                ("n_spheres", C.c_uint32), ("n_tripars", C.c_uint32), ("n_lights", C.c_uint32),
+                ("n_list_surfaces", C.c_uint64), ("origin", C.c_float * 3), ("size", C.c_float),
+                ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("horizon", C.c_float),
+                ("device_bytes", C.c_uint64), ("build_ms", C.c_double)]
+
+
+class SnogRenderStats(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("device_ms", C.c_double), ("waves", C.c_uint32), ("kernel_launches", C.c_uint32)]
+
+
+def _sig(name, res, *args):
+    try:
+        f = getattr(_lib, name)
+    except AttributeError:
+        def missing(*_a, _name=name):
+            raise SnogError(SNOG_EINVAL, f"{_name} is not exported by {LIB_PATH}")
+        return missing
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_P = C.c_void_p
+_lib_version = _sig("snog_version", C.c_char_p)
+_last_error = _sig("snog_last_error", C.c_char_p)
+_init = _sig("snog_init", C.c_int, C.c_int)
+_scene_create = _sig("snog_scene_create", C.c_int, C.POINTER(SnogSceneDesc), C.POINTER(_P))
+_scene_build_host = _sig("snog_scene_build_host", C.c_int, C.POINTER(SnogSceneDesc), C.POINTER(_P))
+_scene_destroy = _sig("snog_scene_destroy", C.c_int, _P)
+_scene_info = _sig("snog_scene_info", C.c_int, _P, C.POINTER(SnogSceneInfo))
+_scene_octree = _sig("snog_scene_octree", C.c_int, _P, _P, _P, _P)
+_trace = _sig("snog_trace", C.c_int, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P)
+_trace_device = _sig("snog_trace_device", C.c_int, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P)
+_render = _sig("snog_render", C.c_int, _P, C.POINTER(SnogCamera), C.POINTER(SnogRenderParams), _P,
+               C.POINTER(SnogRenderStats))
+_render_device = _sig("snog_render_device", C.c_int, _P, C.POINTER(SnogCamera),
+                      C.POINTER(SnogRenderParams), _P, _P, C.POINTER(SnogRenderStats))
+
+
+def _check(rc):
+    if rc != SNOG_OK:
+        raise SnogError(rc, _last_error().decode(errors="replace"))
+
+
+def version():
+    return _lib_version().decode()
+
+
+def init(device=0):
+    _check(_init(device))
+
+
+def _ptr(a):
+    return None if a is None or a.size == 0 else a.ctypes.data
+
+
+def camera_struct(cam: Camera) -> SnogCamera:
+    c = SnogCamera()
+    for name in ("pos", "forward", "right", "up"):
+        getattr(c, name)[:] = [float(x) for x in np.asarray(getattr(cam, name), np.float32)]
+    c.tan_half_fov_x = cam.tan_half_fov_x
+    c.tan_half_fov_y = cam.tan_half_fov_y
+    return c
+
+
+def params_struct(p: RenderParams) -> SnogRenderParams:
+    return SnogRenderParams(p.width, p.height, p.spp, p.min_path_len, p.max_path_len,
+                            p.direct_samples, p.min_trace, p.bg_alpha, p.seed)
+
+
+class Scene:
+    """A scene resident on the device (or host-only, for inspecting the
+    octree).  Mirrors the reference's GlobalRenderState/Scene pair: built
+    once from the surfaces and lights, then rendered or traced."""
+
+    def __init__(self, data: SceneData, device=True):
+        self.data = data
+        keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dt)
+            keep.append(a)
+            return a
+
+        d = SnogSceneDesc()
+        m = arr(data.materials, data.materials.dtype)
+        d.n_materials, d.materials = len(m), _ptr(m)
+        v = arr(data.vertices, np.float32)
+        d.n_vertices, d.vertices = len(data.vertices), _ptr(v)
+        t = arr(data.triangles, np.uint32)
+        tm = arr(data.tri_mat, np.uint32)
+        d.n_triangles, d.triangles, d.tri_material = len(data.triangles), _ptr(t), _ptr(tm)
+        s = arr(data.spheres, data.spheres.dtype)
+        d.n_spheres, d.spheres = len(s), _ptr(s)
+        tp = arr(data.tripars, data.tripars.dtype)
+        d.n_tripars, d.tripars = len(tp), _ptr(tp)
+        pl = arr(data.point_lights, data.point_lights.dtype)
+        d.n_point_lights, d.point_lights = len(pl), _ptr(pl)
+        fl = arr(data.far_lights, data.far_lights.dtype)
+        d.n_far_lights, d.far_lights = len(fl), _ptr(fl)
+        if data.envmap is not None:
+            e = arr(data.envmap, np.float32)
+            d.env_height, d.env_width = e.shape[0], e.shape[1]
+            d.env_rgb = _ptr(e)
+        d.env_frame[:] = [float(x) for x in np.asarray(data.env_frame, np.float32).reshape(9)]
+        h = _P()
+        _check((_scene_create if device else _scene_build_host)(C.byref(d), C.byref(h)))
+        self._h = h
+        self.on_device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(_scene_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        i = SnogSceneInfo()
+        _check(_scene_info(self._h, C.byref(i)))
+        return {f: (list(getattr(i, f)) if isinstance(getattr(i, f), C.Array) else getattr(i, f))
+                for f, _ in SnogSceneInfo._fields_}
+
+    def octree(self):
+        """(origin, size, children[n,8], heads[n], plist) with plist entries as
+        primitive ids, -1 ending each list -- the reference's Octree arrays."""
+        inf = self.info()
+        ch = np.zeros((inf["n_nodes"], 8), np.uint32)
+        hd = np.zeros(inf["n_nodes"], np.uint32)
+        pl = np.zeros(inf["n_plist"], np.int32)
+        _check(_scene_octree(self._h, _ptr(ch), _ptr(hd), _ptr(pl)))
+        return {"origin": np.array(inf["origin"], np.float32), "size": inf["size"],
+                "children": ch, "heads": hd, "list": pl}
+
+    def trace(self, rays_soa, n_closest, want_normal=False):
+        """Closest/any-hit queries for a (7, n) float32 SoA batch in host
+        memory.  Returns (prim, t, normal or None, counters)."""
+        rays = np.ascontiguousarray(rays_soa, np.float32)
+        n = rays.shape[1]
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        nrm = np.empty((n, 3), np.float32) if want_normal else None
+        cnt = np.zeros(4, np.uint64)
+        _check(_trace(self._h, _ptr(rays), n, n_closest, _ptr(prim), _ptr(t), _ptr(nrm), _ptr(cnt)))
+        return prim, t, nrm, {"closest_nodes": int(cnt[0]), "closest_tests": int(cnt[1]),
+                              "any_nodes": int(cnt[2]), "any_tests": int(cnt[3])}
+
+    def trace_device(self, d_rays, n, n_closest, d_prim, d_t=None, d_normal=None, stream=None):
+        """Device-pointer variant (integers, e.g. torch tensor .data_ptr())."""
+        _check(_trace_device(self._h, d_rays, n, n_closest, d_prim, d_t, d_normal, stream))
+
+    def render(self, camera: Camera, params: RenderParams):
+        """Render to a (height, width, 3) float32 image in host memory."""
+        out = np.empty((params.height, params.width, 3), np.float32)
+        st = SnogRenderStats()
+        cs, ps = camera_struct(camera), params_struct(params)
+        _check(_render(self._h, C.byref(cs), C.byref(ps), _ptr(out), C.byref(st)))
+        return out, {f: getattr(st, f) for f, _ in SnogRenderStats._fields_}
+
+    def render_device(self, camera: Camera, params: RenderParams, d_out, stream=None,
+                      want_stats=False):
+        st = SnogRenderStats()
+        cs, ps = camera_struct(camera), params_struct(params)
+        _check(_render_device(self._h, C.byref(cs), C.byref(ps), d_out, stream,
+                              C.byref(st) if want_stats else None))
+        return {f: getattr(st, f) for f, _ in SnogRenderStats._fields_} if want_stats else None
+
+
+def exported_symbols():
+    """Names declared in include/snogray_b200.h (for the ABI check)."""
+    import re
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "snogray_b200.h")
+    with open(hdr) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"^\w[\w\s\*]*?\b(snog_\w+)\s*\(", text, re.M)))
+
+
+__all__ = ["Scene", "SceneData", "Camera", "RenderParams", "SnogError", "scenes", "init",
+           "version", "exported_symbols", "LIB_PATH"]

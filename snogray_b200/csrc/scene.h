@@ -1,0 +1,51 @@
+// scene.h -- the library-side scene object behind the SnogScene handle.
+
+#ifndef SNOG_SCENE_H
+#define SNOG_SCENE_H
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/snogray_b200.h"
+#include "octree_build.h"
+#include "snog_common.h"
+
+namespace snog {
+
+// Device allocations owned by one scene.
+struct DeviceArena {
+  std::vector<void *> blocks;
+  uint64_t bytes = 0;
+  void *alloc(size_t n);           // throws CudaError on failure
+  void *upload(const void *src, size_t n);
+  void release();
+};
+
+struct SceneImpl {
+  std::mutex mu;
+  int device = 0;
+  OctreeArrays oct;                 // host copy (export, stats)
+  DevScene dev{};                   // device view passed to kernels
+  DeviceArena arena;
+  SnogSceneInfo info{};
+  uint32_t n_tri = 0, n_sph = 0, n_tpar = 0;
+  // host copies needed by the host side of rendering
+  float bbox_min[3], bbox_max[3];
+  bool on_device = false;
+};
+
+// Build and upload; throws snog::Error on failure.
+SceneImpl *build_scene(const SnogSceneDesc &desc, bool upload = true);
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+void check_cuda(int err, const char *what);   // throws Error{SNOG_ECUDA}
+
+}  // namespace snog
+
+#endif

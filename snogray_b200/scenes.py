@@ -1,0 +1,371 @@
+"""Scene data and the seeded synthetic workloads the renderer is measured on.
+
+A `SceneData` holds a scene as flat numpy arrays, in the shape the C ABI's
+`SnogSceneDesc` takes them (include/snogray_b200.h).  Primitive ids follow the
+reference's order of insertion into the acceleration structure
+(surface/surface-group.cc:66-71, surface/mesh.cc:1093-1108): mesh triangles by
+part, then spheres, then tripars.
+
+Material records mirror the reference constructors:
+  Lambert(color)                               material/lambert.h
+  CookTorrance(color, gloss_color, m, ior)     material/cook-torrance.h:27-30
+  Mirror(ior, reflectance, color)              material/mirror.h:47-49
+  Glass(Medium(ior, absorb))                   material/glass.h:27, medium.h:30
+  Glow(color[, underlying])                    material/glow.h:28-30
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+MAT_LAMBERT, MAT_COOK_TORRANCE, MAT_MIRROR, MAT_GLASS, MAT_GLOW = range(5)
+
+# One material record: type, color[3], gloss[3], m, ior_n, ior_k, absorb[3],
+# underlying.  Stored as a structured array so it can be handed to C as-is.
+MAT_DTYPE = np.dtype([("type", "<u4"), ("color", "<f4", 3), ("gloss", "<f4", 3),
+                      ("m", "<f4"), ("ior_n", "<f4"), ("ior_k", "<f4"),
+                      ("absorb", "<f4", 3), ("underlying", "<i4")])
+SPHERE_DTYPE = np.dtype([("center", "<f4", 3), ("radius", "<f4"), ("mat", "<u4")])
+TRIPAR_DTYPE = np.dtype([("v0", "<f4", 3), ("e1", "<f4", 3), ("e2", "<f4", 3),
+                         ("parallelogram", "<u4"), ("mat", "<u4")])
+PLIGHT_DTYPE = np.dtype([("pos", "<f4", 3), ("color", "<f4", 3), ("angle", "<f4"),
+                         ("fringe_angle", "<f4"), ("dir", "<f4", 3)])
+FLIGHT_DTYPE = np.dtype([("dir", "<f4", 3), ("angle", "<f4"), ("color", "<f4", 3)])
+
+
+def _f32(x):
+    return np.float32(x)
+
+
+@dataclass
+class Camera:
+    """Pinhole camera in the reference's representation (camera/camera.h).
+
+    `point()` and `set_vert_fov()` follow Camera::_point (camera.h:114-128) and
+    Camera::set_fov (camera.h:231-242) for a film format of the image's aspect
+    ratio, in float32 like the reference's dist_t.
+    """
+    pos: np.ndarray = field(default_factory=lambda: np.zeros(3, np.float32))
+    forward: np.ndarray = field(default_factory=lambda: np.array([0, 0, 1], np.float32))
+    right: np.ndarray = field(default_factory=lambda: np.array([1, 0, 0], np.float32))
+    up: np.ndarray = field(default_factory=lambda: np.array([0, 1, 0], np.float32))
+    tan_half_fov_x: float = 0.0
+    tan_half_fov_y: float = 0.0
+
+    @staticmethod
+    def _unit(v):
+        v = np.asarray(v, np.float32)
+        return (v * _f32(1.0 / np.float32(np.sqrt(np.float32(np.dot(v, v)))))).astype(np.float32)
+
+    def move(self, pos):
+        self.pos = np.asarray(pos, np.float32)
+
+    def point(self, target, user_up):
+        d = self._unit(np.asarray(target, np.float32) - self.pos)
+        user_up = np.asarray(user_up, np.float32)
+        self.forward = d
+        self.right = self._unit(np.cross(user_up, d))
+        self.up = self._unit(np.cross(d, self.right))
+
+    def set_vert_fov(self, fov, aspect):
+        t = math.tan(fov / 2)
+        self.tan_half_fov_y = float(_f32(t))
+        self.tan_half_fov_x = float(_f32(t * aspect))
+
+
+@dataclass
+class SceneData:
+    materials: np.ndarray
+    vertices: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+    triangles: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.uint32))
+    tri_mat: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+    spheres: np.ndarray = field(default_factory=lambda: np.zeros(0, SPHERE_DTYPE))
+    tripars: np.ndarray = field(default_factory=lambda: np.zeros(0, TRIPAR_DTYPE))
+    point_lights: np.ndarray = field(default_factory=lambda: np.zeros(0, PLIGHT_DTYPE))
+    far_lights: np.ndarray = field(default_factory=lambda: np.zeros(0, FLIGHT_DTYPE))
+    envmap: np.ndarray | None = None          # (H, W, 3) float32, row 0 = top
+    env_frame: np.ndarray = field(default_factory=lambda: np.eye(3, dtype=np.float32))
+    name: str = "scene"
+
+    def __post_init__(self):
+        self.vertices = np.ascontiguousarray(self.vertices, np.float32).reshape(-1, 3)
+        self.triangles = np.ascontiguousarray(self.triangles, np.uint32).reshape(-1, 3)
+        self.tri_mat = np.ascontiguousarray(self.tri_mat, np.uint32).reshape(-1)
+        if self.tri_mat.size and np.any(np.diff(self.tri_mat.astype(np.int64)) < 0):
+            raise ValueError("tri_mat must be non-decreasing (one mesh part per material run)")
+        if self.envmap is not None:
+            self.envmap = np.ascontiguousarray(self.envmap, np.float32)
+
+    @property
+    def n_prims(self):
+        return len(self.triangles) + len(self.spheres) + len(self.tripars)
+
+
+@dataclass
+class RenderParams:
+    """ValTable keys of the reference's path integrator and image output
+    (render/path-integ.cc:64-68, render-params.h:32-36,
+    global-render-state.cc:37-38)."""
+    width: int = 256
+    height: int = 256
+    spp: int = 16                      # samples
+    min_path_len: int = 3              # surface_integ.min_path_len
+    max_path_len: int = 25             # surface_integ.max_path_len
+    direct_samples: int = 1            # surface_integ.direct_samples
+    min_trace: float = 1e-3            # min_trace
+    bg_alpha: float = 1.0              # background_alpha
+    seed: int = 0
+
+
+def material(mtype, color=(0, 0, 0), gloss=(1, 1, 1), m=0.0, ior_n=1.5, ior_k=0.0,
+             absorb=(0, 0, 0), underlying=-1):
+    r = np.zeros((), MAT_DTYPE)
+    r["type"], r["color"], r["gloss"], r["m"] = mtype, color, gloss, m
+    r["ior_n"], r["ior_k"], r["absorb"], r["underlying"] = ior_n, ior_k, absorb, underlying
+    return r
+
+
+def _mats(recs):
+    return np.array([r[()] for r in recs], MAT_DTYPE)
+
+
+# ---------------------------------------------------------------------------
+# Cornell-style box: 5 axis-aligned quads (10 triangles, 3 Lambert parts), a
+# Lambert sphere and a Glass sphere of radius 0.3, and a 0.25 x 0.25
+# parallelogram area light of radiance 15 just below the ceiling.
+
+def cornell_box():
+    mats = _mats([
+        material(MAT_LAMBERT, (0.73, 0.73, 0.73)),   # 0 white
+        material(MAT_LAMBERT, (0.65, 0.05, 0.05)),   # 1 red
+        material(MAT_LAMBERT, (0.12, 0.45, 0.15)),   # 2 green
+        material(MAT_GLASS, ior_n=1.5),              # 3 glass, Medium(1.5)
+        material(MAT_GLOW, (15.0, 15.0, 15.0)),      # 4 light
+    ])
+    v = np.array([[0, 0, 0], [1, 0, 0], [1, 0, 1], [0, 0, 1],      # floor y=0
+                  [0, 1, 0], [1, 1, 0], [1, 1, 1], [0, 1, 1]],     # ceiling y=1
+                 np.float32)
+    tris = np.array([
+        [0, 1, 2], [0, 2, 3],      # floor
+        [4, 6, 5], [4, 7, 6],      # ceiling
+        [3, 2, 6], [3, 6, 7],      # back wall z=1
+        [0, 3, 7], [0, 7, 4],      # left wall x=0 (red)
+        [1, 5, 6], [1, 6, 2],      # right wall x=1 (green)
+    ], np.uint32)
+    tri_mat = np.array([0, 0, 0, 0, 0, 0, 1, 1, 2, 2], np.uint32)
+    spheres = np.zeros(2, SPHERE_DTYPE)
+    spheres[0] = ((0.3, 0.3, 0.65), 0.3, 0)
+    spheres[1] = ((0.7, 0.6, 0.3), 0.3, 3)
+    tripars = np.zeros(1, TRIPAR_DTYPE)
+    # normal = e2 x e1 (surface/tripar.cc:54) points down, into the room.
+    tripars[0] = ((0.375, 0.999, 0.375), (0, 0, 0.25), (0.25, 0, 0), 1, 4)
+    return SceneData(materials=mats, vertices=v, triangles=tris, tri_mat=tri_mat,
+                     spheres=spheres, tripars=tripars, name="cornell")
+
+
+def cornell_camera(width, height):
+    cam = Camera()
+    cam.move((0.5, 0.5, -1.2))
+    cam.point((0.5, 0.5, 0.5), (0, 1, 0))
+    cam.set_vert_fov(math.radians(40.0), width / height)
+    return cam
+
+
+def cornell_params(width=256, height=256, spp=16, seed=0):
+    return RenderParams(width=width, height=height, spp=spp, min_path_len=3, max_path_len=8,
+                        direct_samples=1, seed=seed)
+
+
+# ---------------------------------------------------------------------------
+# Random triangle soup: centroids U[0,1]^3, edge lengths U(lo, hi), random
+# orientation.
+
+def _random_rotations(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    r = np.empty((n, 3, 3))
+    r[:, 0, 0] = 1 - 2 * (y * y + z * z); r[:, 0, 1] = 2 * (x * y - z * w); r[:, 0, 2] = 2 * (x * z + y * w)
+    r[:, 1, 0] = 2 * (x * y + z * w); r[:, 1, 1] = 1 - 2 * (x * x + z * z); r[:, 1, 2] = 2 * (y * z - x * w)
+    r[:, 2, 0] = 2 * (x * z - y * w); r[:, 2, 1] = 2 * (y * z + x * w); r[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return r
+
+
+def random_triangles(n, seed=2, edge_lo=0.002, edge_hi=0.02, mats=None):
+    """n random triangles as one mesh of one part (material 0)."""
+    rng = np.random.default_rng(seed)
+    cent = rng.uniform(0, 1, size=(n, 3))
+    # Two edges from the first vertex, lengths U(lo, hi), at a random angle in
+    # the triangle's plane, then a random rotation.
+    l1 = rng.uniform(edge_lo, edge_hi, n)
+    l2 = rng.uniform(edge_lo, edge_hi, n)
+    ang = rng.uniform(0.3, math.pi - 0.3, n)
+    e1 = np.stack([l1, np.zeros(n), np.zeros(n)], 1)
+    e2 = np.stack([l2 * np.cos(ang), l2 * np.sin(ang), np.zeros(n)], 1)
+    rot = _random_rotations(rng, n)
+    e1 = np.einsum("nij,nj->ni", rot, e1)
+    e2 = np.einsum("nij,nj->ni", rot, e2)
+    v0 = cent - (e1 + e2) / 3
+    verts = np.stack([v0, v0 + e1, v0 + e2], 1).reshape(-1, 3).astype(np.float32)
+    tris = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
+    if mats is None:
+        mats = _mats([material(MAT_LAMBERT, (0.7, 0.7, 0.7))])
+    return SceneData(materials=mats, vertices=verts, triangles=tris,
+                     tri_mat=np.zeros(n, np.uint32), name=f"soup{n}")
+
+
+def random_rays(n, seed=3, lo=-0.1, hi=1.1):
+    """Ray batch: origins U[lo,hi]^3, directions uniform on the sphere, t_max=inf.
+    Returns (n, 7) float32 SoA rows ox oy oz dx dy dz tmax as a (7, n) array."""
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(lo, hi, size=(n, 3))
+    z = rng.uniform(-1, 1, n)
+    phi = rng.uniform(0, 2 * math.pi, n)
+    r = np.sqrt(np.maximum(0, 1 - z * z))
+    d = np.stack([r * np.cos(phi), r * np.sin(phi), z], 1)
+    soa = np.empty((7, n), np.float32)
+    soa[0:3] = o.T
+    soa[3:6] = d.T
+    soa[6] = np.inf
+    return soa
+
+
+# ---------------------------------------------------------------------------
+# Terrain + spheres + procedural sky (z up).
+
+def _value_noise(rng, res, x, y):
+    g = rng.uniform(-1, 1, size=(res + 1, res + 1))
+    xs, ys = x * res, y * res
+    xi = np.clip(np.floor(xs).astype(int), 0, res - 1)
+    yi = np.clip(np.floor(ys).astype(int), 0, res - 1)
+    fx, fy = xs - xi, ys - yi
+    sx, sy = fx * fx * (3 - 2 * fx), fy * fy * (3 - 2 * fy)
+    a = g[xi, yi] * (1 - sx) + g[xi + 1, yi] * sx
+    b = g[xi, yi + 1] * (1 - sx) + g[xi + 1, yi + 1] * sx
+    return a * (1 - sy) + b * sy
+
+
+def fbm_heightfield(n, seed=7, octaves=6, amplitude=0.2):
+    rng = np.random.default_rng(seed)
+    u = np.linspace(0, 1, n)
+    x, y = np.meshgrid(u, u, indexing="ij")
+    h = np.zeros((n, n))
+    amp, freq, norm = 1.0, 4, 0.0
+    for _ in range(octaves):
+        h += amp * _value_noise(rng, freq, x, y)
+        norm += amp
+        amp *= 0.5
+        freq *= 2
+    return (amplitude * h / norm).astype(np.float32)
+
+
+def sky_envmap(w=1024, h=512, sun_elev_deg=35.0, sun_azim_deg=40.0, sigma_deg=1.0, peak=5e3):
+    """Lat-long sky (z up): vertical gradient plus a Gaussian sun."""
+    v = (np.arange(h) + 0.5) / h
+    lat = (0.5 - v) * math.pi                      # row 0 = top = zenith
+    u = (np.arange(w) + 0.5) / w
+    lng = (u - 0.5) * 2 * math.pi
+    lat2, lng2 = np.meshgrid(lat, lng, indexing="ij")
+    # Direction for (lat, lng) in the reference's z-axis lat-long convention
+    # (geometry/spherical-coords.h:157-168): x = cos(lng) cos(lat),
+    # y = -sin(lng) cos(lat), z = sin(lat).
+    d = np.stack([np.cos(lng2) * np.cos(lat2), -np.sin(lng2) * np.cos(lat2), np.sin(lat2)], -1)
+    t = np.clip(np.sin(lat2), 0, 1)[..., None]
+    zenith = np.array([0.25, 0.45, 0.95])
+    horizon = np.array([0.85, 0.9, 1.0])
+    ground = np.array([0.25, 0.22, 0.2])
+    sky = np.where(lat2[..., None] >= 0, horizon * (1 - t) + zenith * t, ground)
+    se, sa = math.radians(sun_elev_deg), math.radians(sun_azim_deg)
+    sdir = np.array([math.cos(sa) * math.cos(se), -math.sin(sa) * math.cos(se), math.sin(se)])
+    ang = np.arccos(np.clip(d @ sdir, -1, 1))
+    sig = math.radians(sigma_deg)
+    sun = peak * np.exp(-0.5 * (ang / sig) ** 2)
+    img = sky + sun[..., None] * np.array([1.0, 0.95, 0.85])
+    return img.astype(np.float32)
+
+
+def terrain_scene(n=1024, n_spheres=200, seed=11, env_w=1024, env_h=512):
+    rng = np.random.default_rng(seed)
+    hf = fbm_heightfield(n, seed=seed)
+    u = np.linspace(0, 1, n, dtype=np.float32)
+    x, y = np.meshgrid(u, u, indexing="ij")
+    verts = np.stack([x, y, hf], -1).reshape(-1, 3).astype(np.float32)
+    i, j = np.meshgrid(np.arange(n - 1), np.arange(n - 1), indexing="ij")
+    a = (i * n + j).ravel()
+    b, c, d = a + n, a + n + 1, a + 1
+    # Counter-clockwise seen from +z; the reference's meshes are left-handed
+    # by default (normal = e2 x e1, surface/mesh.h:55), which is harmless for
+    # shading since frames are flipped to face the viewer.
+    tris = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)]).astype(np.uint32)
+    recs = [material(MAT_LAMBERT, (0.45, 0.4, 0.33))]
+    sph = np.zeros(n_spheres, SPHERE_DTYPE)
+    kinds = rng.choice(3, size=n_spheres, p=[0.6, 0.2, 0.2])
+    for k in range(n_spheres):
+        r = rng.uniform(0.01, 0.05)
+        px, py = rng.uniform(0.05, 0.95, 2)
+        gx, gy = int(px * (n - 1)), int(py * (n - 1))
+        pz = hf[gx, gy] + r + rng.uniform(0.0, 0.05)
+        col = rng.uniform(0.2, 0.9, 3)
+        if kinds[k] == 0:
+            recs.append(material(MAT_COOK_TORRANCE, col, (1, 1, 1), m=rng.uniform(0.05, 0.5),
+                                 ior_n=1.5))
+        elif kinds[k] == 1:
+            recs.append(material(MAT_GLASS, ior_n=1.5))
+        else:
+            recs.append(material(MAT_LAMBERT, col))
+        sph[k] = ((px, py, pz), r, len(recs) - 1)
+    env = sky_envmap(env_w, env_h)
+    return SceneData(materials=_mats(recs), vertices=verts, triangles=tris,
+                     tri_mat=np.zeros(len(tris), np.uint32), spheres=sph, envmap=env,
+                     name=f"terrain{n}")
+
+
+def terrain_camera(width, height):
+    cam = Camera()
+    cam.move((-0.35, -0.3, 0.45))
+    cam.point((0.55, 0.55, 0.0), (0, 0, 1))
+    cam.set_vert_fov(math.radians(45.0), width / height)
+    return cam
+
+
+def terrain_params(width=1920, height=1080, spp=64, seed=0):
+    return RenderParams(width=width, height=height, spp=spp, min_path_len=3, max_path_len=16,
+                        direct_samples=1, seed=seed)
+
+
+# ---------------------------------------------------------------------------
+# Random-soup scene with mixed materials and one area light, for the batched
+# and served workloads.
+
+def soup_scene(n_tris, seed, envmap=None):
+    rng = np.random.default_rng(seed)
+    recs = [material(MAT_LAMBERT, rng.uniform(0.2, 0.8, 3)),
+            material(MAT_COOK_TORRANCE, rng.uniform(0.2, 0.8, 3), (1, 1, 1),
+                     m=rng.uniform(0.05, 0.5), ior_n=1.5),
+            material(MAT_GLOW, (12.0, 12.0, 12.0))]
+    s = random_triangles(n_tris, seed=seed, mats=_mats(recs))
+    # Lambert/Cook-Torrance mix: parts must be contiguous runs.
+    n_ct = int(rng.uniform(0.2, 0.8) * n_tris)
+    s.tri_mat = np.concatenate([np.zeros(n_tris - n_ct, np.uint32), np.ones(n_ct, np.uint32)])
+    tp = np.zeros(1, TRIPAR_DTYPE)
+    tp[0] = ((0.35, 0.35, 1.3), (0.3, 0, 0), (0, 0.3, 0), 1, 2)   # faces -z
+    s.tripars = tp
+    if envmap is not None:
+        s.envmap = envmap
+    s.name = f"soup{n_tris}_s{seed}"
+    return s
+
+
+def orbit_camera(width, height, rng, center=(0.5, 0.5, 0.5), dist=1.8):
+    z = rng.uniform(-0.6, 0.8)
+    phi = rng.uniform(0, 2 * math.pi)
+    r = math.sqrt(1 - z * z)
+    pos = np.array(center) + dist * np.array([r * math.cos(phi), r * math.sin(phi), z])
+    cam = Camera()
+    cam.move(pos)
+    cam.point(center, (0, 0, 1))
+    cam.set_vert_fov(math.radians(50.0), width / height)
+    return cam

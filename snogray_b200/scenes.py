@@ -233,6 +233,42 @@ def random_rays(n, seed=3, lo=-0.1, hi=1.1):
     return soa
 
 
+def mixed_scene(n_tris, n_spheres, n_tripars, seed=5):
+    """Random triangles, spheres (radius U(0.005, 0.05)) and tripars (edge
+    lengths U(0.01, 0.1), half of them parallelograms) in the unit cube."""
+    rng = np.random.default_rng(seed + 1000)
+    s = random_triangles(n_tris, seed=seed)
+    sph = np.zeros(n_spheres, SPHERE_DTYPE)
+    sph["center"] = rng.uniform(0, 1, (n_spheres, 3))
+    sph["radius"] = rng.uniform(0.005, 0.05, n_spheres)
+    tp = np.zeros(n_tripars, TRIPAR_DTYPE)
+    v0 = rng.uniform(0, 1, (n_tripars, 3))
+    rot = _random_rotations(rng, n_tripars)
+    e1 = np.einsum("nij,nj->ni", rot, np.stack([rng.uniform(0.01, 0.1, n_tripars),
+                                                np.zeros(n_tripars), np.zeros(n_tripars)], 1))
+    e2 = np.einsum("nij,nj->ni", rot, np.stack([np.zeros(n_tripars),
+                                                rng.uniform(0.01, 0.1, n_tripars),
+                                                np.zeros(n_tripars)], 1))
+    tp["v0"], tp["e1"], tp["e2"] = v0, e1, e2
+    tp["parallelogram"] = np.arange(n_tripars) % 2
+    s.spheres, s.tripars = sph, tp
+    s.name = f"mixed{n_tris}_{n_spheres}_{n_tripars}_s{seed}"
+    return s
+
+
+def scene_digest(sd):
+    """sha256 over every array of a SceneData (pins fixtures to the exact
+    float32 bits the generator produced)."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in (sd.materials, sd.vertices, sd.triangles, sd.tri_mat, sd.spheres, sd.tripars,
+              sd.point_lights, sd.far_lights):
+        h.update(np.ascontiguousarray(a).tobytes())
+    if sd.envmap is not None:
+        h.update(np.ascontiguousarray(sd.envmap).tobytes())
+    return h.hexdigest()
+
+
 # ---------------------------------------------------------------------------
 # Terrain + spheres + procedural sky (z up).
 

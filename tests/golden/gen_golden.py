@@ -1,0 +1,175 @@
+"""Generate the golden fixtures in tests/golden/ from the snogray reference.
+
+Runs the reference renderer compiled in place from its own sources
+(oracle/_ref/snog_ref_parity: -O2 -ffp-contract=off, IEEE single precision in
+source order) through its own C++ API (oracle/ref_harness.cc).  The reference
+tree exists only on the development machine, so the outputs are committed;
+the GPU box and the CPU test suite read them.
+
+Each scene is regenerated at test time from its generator and seed and pinned
+by a sha256 digest of its arrays, so the fixtures hold only ids, distances,
+octree digests and image statistics, not geometry.
+
+    python tests/golden/gen_golden.py            # all fixtures
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from snogray_b200 import scenes  # noqa: E402
+import spec  # noqa: E402
+
+
+def edge_rays(sd, n_rand, seed):
+    """Rays that exercise the corners of the traversal: axis-aligned and
+    zero directions, origins on the root cube's planes, zero and short
+    extents, plus random rays."""
+    rng = np.random.default_rng(seed)
+    rays = [scenes.random_rays(n_rand, seed=seed)]
+    lo = sd.vertices.min(0) if len(sd.vertices) else np.zeros(3)
+    hi = sd.vertices.max(0) if len(sd.vertices) else np.ones(3)
+    k = 512
+    o = rng.uniform(lo - 0.05, hi + 0.05, (k, 3)).astype(np.float32)
+    axes = np.eye(3, dtype=np.float32)
+    d = np.concatenate([axes, -axes])[rng.integers(0, 6, k)]
+    soa = np.empty((7, k), np.float32)
+    soa[0:3], soa[3:6], soa[6] = o.T, d.T, np.inf
+    rays.append(soa)
+    # origins snapped to the octree midplanes of the unit cube
+    o2 = rng.uniform(0, 1, (k, 3)).astype(np.float32)
+    o2[:, rng.integers(0, 3)] = 0.5
+    dd = rng.normal(size=(k, 3)).astype(np.float32)
+    dd /= np.linalg.norm(dd, axis=1, keepdims=True)
+    soa2 = np.empty((7, k), np.float32)
+    soa2[0:3], soa2[3:6] = o2.T, dd.T
+    soa2[6] = np.where(np.arange(k) % 4 == 0, 0.0, np.where(np.arange(k) % 4 == 1, 0.05, np.inf))
+    rays.append(soa2)
+    z = np.zeros((7, 16), np.float32)       # zero directions
+    z[0:3] = rng.uniform(0, 1, (3, 16))
+    z[6] = np.inf
+    rays.append(z)
+    return np.concatenate(rays, axis=1)
+
+
+def camera_rays(cam, w, h, max_trace, seed):
+    """Eye rays as Camera::eye_ray makes them for jittered film positions
+    (camera/camera.cc:108-160): unnormalised direction, t1 = max_trace."""
+    rng = np.random.default_rng(seed)
+    n = w * h
+    px = (np.arange(n) % w + rng.uniform(0, 1, n)).astype(np.float32)
+    py = (np.arange(n) // w + rng.uniform(0, 1, n)).astype(np.float32)
+    u = px / np.float32(w)
+    v = (np.float32(h) - py) / np.float32(h)
+    x = (np.float32(2) * u - np.float32(1)).astype(np.float32)
+    y = (np.float32(2) * v - np.float32(1)).astype(np.float32)
+    f, r, up = (np.asarray(a, np.float32) for a in (cam.forward, cam.right, cam.up))
+    d = (f[None] + (r[None] * x[:, None]) * np.float32(cam.tan_half_fov_x)
+         + (up[None] * y[:, None]) * np.float32(cam.tan_half_fov_y)).astype(np.float32)
+    soa = np.empty((7, n), np.float32)
+    soa[0:3] = np.asarray(cam.pos, np.float32)[:, None]
+    soa[3:6] = d.T
+    soa[6] = max_trace
+    return soa
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+TRACE_CASES = {
+    # name: (scene factory, ray factory, n_closest fraction)
+    "mixed": (lambda: scenes.mixed_scene(4000, 300, 200, seed=5),
+              lambda sd: edge_rays(sd, 12000, seed=31)),
+    "soup": (lambda: scenes.random_triangles(20000, seed=2),
+             lambda sd: scenes.random_rays(16384, seed=3)),
+    "terrain": (lambda: scenes.terrain_scene(n=96, n_spheres=40, seed=11, env_w=64, env_h=32),
+                lambda sd: edge_rays(sd, 8000, seed=37)),
+    "cornell_camera": (lambda: scenes.cornell_box(),
+                       lambda sd: camera_rays(scenes.cornell_camera(64, 64), 64, 64,
+                                              np.float32(4.0), seed=41)),
+}
+
+
+def gen_trace(name):
+    make_scene, make_rays = TRACE_CASES[name]
+    sd = make_scene()
+    rays = make_rays(sd)
+    n = rays.shape[1]
+    n_closest = n // 2
+    prim, t, nrm, stats, _ = spec.ref_trace(sd, rays, n_closest, threads=8)
+    oc = spec.ref_octree(sd)
+    hit = np.nonzero(prim[:n_closest] >= 0)[0]
+    np.savez_compressed(
+        os.path.join(HERE, f"trace_{name}.npz"), prim=prim, t=t, normal_hit=nrm[hit],
+        closest_nodes=stats["closest"]["node_calls"], any_nodes=stats["any"]["node_calls"],
+        scene_digest=scenes.scene_digest(sd), rays_digest=digest(rays), n_closest=n_closest,
+        oct_children_digest=digest(oc["children"]), oct_heads_digest=digest(oc["heads"]),
+        oct_list_digest=digest(oc["list"]), oct_origin=oc["origin"], oct_size=oc["size"],
+        oct_nodes=len(oc["heads"]))
+    hit = (prim[:n_closest] >= 0).mean(), (prim[n_closest:] >= 0).mean()
+    print(f"trace_{name}: {n} rays, hit rate closest {hit[0]:.3f} any {hit[1]:.3f}, "
+          f"{len(oc['heads'])} nodes")
+
+
+def image_stats(imgs):
+    """Per-channel image means over K independent renders and their standard
+    error (snogdiff's mean, snogdiff.cc:133-190)."""
+    means = np.array([im.reshape(-1, 3).mean(0) for im in imgs])
+    return means.mean(0), means.std(0, ddof=1) / math.sqrt(len(imgs))
+
+
+RENDER_CASES = {
+    "cornell": (scenes.cornell_box, scenes.cornell_camera, scenes.cornell_params, 64, 64, 16),
+    "terrain": (lambda: scenes.terrain_scene(n=96, n_spheres=40, seed=11, env_w=256, env_h=128),
+                scenes.terrain_camera, scenes.terrain_params, 64, 48, 16),
+}
+
+
+def gen_render(name, k=16, gt_spp=4096):
+    make_scene, make_cam, make_params, w, h, spp = RENDER_CASES[name]
+    sd = make_scene()
+    cam = make_cam(w, h)
+    params = make_params(w, h, spp)
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(8) as ex:
+        futs = [ex.submit(spec.ref_render, sd, cam, params, 1, i) for i in range(k)]
+        res = [f.result() for f in futs]
+    imgs = [r[0] for r in res]
+    mean, se = image_stats(imgs)
+    gt, info = spec.ref_render(sd, cam, params, threads=8, seed_skip=1000, spp=gt_spp)
+    # RMSE of each spp-S reference render against the ground truth.
+    rmse = np.array([np.sqrt(((im - gt) ** 2).mean()) for im in imgs])
+    np.savez_compressed(os.path.join(HERE, f"render_{name}.npz"),
+                        mean=mean, se=se, rmse=rmse, gt=gt.astype(np.float16), k=k, spp=spp,
+                        gt_spp=gt_spp, width=w, height=h, scene_digest=scenes.scene_digest(sd),
+                        ref_mpaths=np.array([r[1]["mpaths_per_s"] for r in res]))
+    print(f"render_{name}: mean {mean} se {se} rmse {rmse.mean():.4f}+-{rmse.std():.4f} "
+          f"gt {info['seconds']:.1f}s")
+
+
+if __name__ == "__main__":
+    if not spec.have_ref():
+        spec.build(["ref"])
+    which = sys.argv[1:] or ["trace", "render"]
+    if "trace" in which:
+        for nm in TRACE_CASES:
+            gen_trace(nm)
+    if "render" in which:
+        for nm in RENDER_CASES:
+            gen_render(nm)
+    with open(os.path.join(HERE, "README.txt"), "w") as f:
+        f.write("Golden fixtures made by tests/golden/gen_golden.py from the snogray reference\n"
+                "compiled in place (oracle/Makefile, parity flavour).  Regenerate with:\n"
+                "    python tests/golden/gen_golden.py\n")

@@ -1,0 +1,83 @@
+"""The product's octree builder against the reference's octree.
+
+The node arrays (BFS order, children, list heads), the packed surface lists,
+the root cube origin and size must be the reference's exactly
+(space/octree-builder.cc:173-650): hit ids depend on them.  Golden digests come
+from the reference compiled in place (tests/golden/gen_golden.py); when the
+compiled reference is present it is also run live on further scenes.
+"""
+
+import hashlib
+
+import numpy as np
+import pytest
+
+import spec
+from gen_golden import TRACE_CASES
+from snogray_b200 import Scene, scenes
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", sorted(TRACE_CASES))
+def test_octree_matches_reference_fixture(name, golden):
+    g = golden(f"trace_{name}.npz")
+    sd = TRACE_CASES[name][0]()
+    assert scenes.scene_digest(sd) == str(g["scene_digest"]), "scene generator drifted"
+    with Scene(sd, device=False) as sc:
+        oc = sc.octree()
+        info = sc.info()
+    assert len(oc["heads"]) == int(g["oct_nodes"])
+    assert np.array_equal(oc["origin"], g["oct_origin"])
+    assert np.float32(oc["size"]) == np.float32(g["oct_size"])
+    assert _digest(oc["children"]) == str(g["oct_children_digest"])
+    assert _digest(oc["heads"]) == str(g["oct_heads_digest"])
+    assert _digest(oc["list"]) == str(g["oct_list_digest"])
+    assert info["max_depth"] >= 1
+
+
+LIVE = [
+    lambda: scenes.cornell_box(),
+    lambda: scenes.random_triangles(3000, seed=17, edge_lo=0.0, edge_hi=0.3),
+    lambda: scenes.mixed_scene(500, 500, 500, seed=23),
+    lambda: scenes.soup_scene(5000, 4),
+    lambda: scenes.terrain_scene(n=48, n_spheres=10, seed=3, env_w=32, env_h=16),
+]
+
+
+@pytest.mark.skipif(not spec.have_ref(), reason="compiled reference not present")
+@pytest.mark.parametrize("k", range(len(LIVE)))
+def test_octree_matches_live_reference(k):
+    sd = LIVE[k]()
+    ref = spec.ref_octree(sd)
+    with Scene(sd, device=False) as sc:
+        mine = sc.octree()
+    for key in ("children", "heads", "list", "origin"):
+        assert np.array_equal(ref[key], mine[key]), key
+    assert np.float32(ref["size"]) == np.float32(mine["size"])
+
+
+def test_degenerate_triangles_left_out():
+    # A zero-area triangle is not inserted (surface/mesh.cc:833-846).
+    sd = scenes.random_triangles(50, seed=1)
+    v = sd.vertices.copy()
+    v[5] = v[3]                                  # triangle 1 collapses to a segment
+    sd.vertices = v
+    with Scene(sd, device=False) as sc:
+        oc = sc.octree()
+    assert 1 not in set(oc["list"].tolist())
+    assert 0 in set(oc["list"].tolist())
+
+
+def test_empty_scene_rejected():
+    sd = scenes.cornell_box()
+    sd.vertices = np.zeros((0, 3), np.float32)
+    sd.triangles = np.zeros((0, 3), np.uint32)
+    sd.tri_mat = np.zeros(0, np.uint32)
+    sd.spheres = sd.spheres[:0]
+    sd.tripars = sd.tripars[:0]
+    import snogray_b200 as sb
+    with pytest.raises(sb.SnogError):
+        Scene(sd, device=False)

@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Throughput of the path-tracing hot path on B200: Mpaths/s.
+
+Workload (one "step" = one whole render job): the seeded terrain scene --
+1024x1024 fBm heightfield (2,093,058 triangles) + 200 spheres (60% Cook-
+Torrance, 20% Glass, 20% Lambert) lit by a 1024x512 procedural sky envmap with
+a Gaussian sun -- rendered at 1920x1080, 64 spp, max path length 16, Mitchell
+filter.  Paths counted = width x height x spp (132,710,400 per step), as the
+reference's own rate (paths rendered in the filter margin are extra work not
+counted).  Synthetic data: the scene is generated from fixed seeds.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device time (CUDA events on the render stream, inputs resident in
+HBM); `e2e` is the same metric through the public host API (snog_render: job
+description in from host memory, the finished image copied back to host
+memory every step), wall clock.  The path state and queues of a wave (~1.2 GB)
+exceed the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: the path shards trivially (independent paths); each rank renders
+its own job replica (weak scaling), no collective on the data path.  Rank 0
+prints one JSON line; timings are the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+WIDTH, HEIGHT, SPP, MAX_LEN = 1920, 1080, 64, 16
+METRIC = "Mpaths/s at matched RMSE (terrain 1920x1080, 64 spp, depth 16)"
+
+
+def workload():
+    from snogray_b200 import scenes
+    sd = scenes.terrain_scene()
+    cam = scenes.terrain_camera(WIDTH, HEIGHT)
+    return sd, cam
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for ln in f:
+                p = [x.strip() for x in ln.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference (CPU) runs: the snogray renderer compiled from its own sources
+
+def ref_available():
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import spec
+    return spec.have_ref("base"), spec
+
+
+def run_reference(sd, cam, params, spp, repeat, threads, rows=0, row0=0):
+    """Render with the reference (baseline flavour: the reference's own
+    optimisation flags) REPEAT times in one process; returns the per-render
+    JSON records."""
+    _, spec = ref_available()
+    with tempfile.TemporaryDirectory() as d:
+        sp, op = os.path.join(d, "s.spec"), os.path.join(d, "o.pfm")
+        spec.write_spec(sp, sd, cam, params)
+        out = subprocess.run([spec.ref_binary("base"), "render", sp, op, str(threads), "0",
+                              str(spp), str(row0), str(rows), str(repeat)],
+                             capture_output=True, text=True, timeout=3600)
+        if out.returncode != 0:
+            raise RuntimeError(out.stderr[-2000:])
+    return [json.loads(ln) for ln in out.stdout.splitlines() if ln.startswith("{")]
+
+
+def algorithmic_bytes_per_ray(rec):
+    """Bytes one query must touch by the reference's own traversal counts
+    (node visits, surface tests, list entries incl. negative-cache hits):
+    28 B ray in + 8 B hit out + 36 B per node (8 child ids + list head)
+    + 4 B per list entry + 36 B per primitive test (three float3)."""
+    nc = max(rec["scene_intersect_calls"], 1)
+    ns = max(rec["scene_shadow_tests"], 1)
+    closest = 36 + (36 * rec["node_calls"] + 4 * (rec["surface_tests"] + rec["neg_cache_hits"])
+                    + 36 * rec["surface_tests"]) / nc
+    shadow = 36 + (36 * rec["shadow_node_calls"]
+                   + 4 * (rec["shadow_surface_tests"] + rec["shadow_neg_cache_hits"])
+                   + 36 * rec["shadow_surface_tests"]) / ns
+    return closest, shadow
+
+
+# ---------------------------------------------------------------------------
+
+def bench_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    ok, _ = ref_available()
+    if not ok:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "compiled reference (oracle/_ref/snog_ref_base) not present"}))
+        return 0
+    from snogray_b200 import scenes
+    sd, cam = workload()
+    params = scenes.terrain_params(WIDTH, HEIGHT, SPP)
+    threads = os.cpu_count() or 1
+    spp_sample = 1
+    recs = run_reference(sd, cam, params, spp_sample, args.warmup + args.steps, threads)
+    timed = recs[args.warmup:]
+    secs = sum(r["seconds"] for r in timed)
+    paths = sum(r["paths"] for r in timed)
+    value = paths / secs * 1e-6
+    ms_per_step = secs / len(timed) * 1e3
+    sample = f"{WIDTH}x{HEIGHT} at {spp_sample} spp per step (of {SPP}), all rows"
+    line = {"metric": METRIC, "value": round(value, 4), "unit": "Mpaths/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "terrain-2M-tris+200-spheres+sky-envmap", "width": WIDTH,
+                       "height": HEIGHT, "spp": SPP, "max_path_len": MAX_LEN,
+                       "sample_spp_per_step": spp_sample},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mpaths/s", "cores": threads,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def bench_ours(args):
+    import ctypes
+
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    import snogray_b200 as sb
+    from snogray_b200 import scenes
+    sb.init(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    sd, cam = workload()
+    scene = sb.Scene(sd)
+    params = scenes.terrain_params(WIDTH, HEIGHT, SPP, seed=1 + rank)
+    out = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+
+    def step(want_stats=False):
+        return scene.render_device(cam, params, out.data_ptr(), sptr, want_stats=want_stats)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: device time on the render stream ------------------
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    for _ in range(args.steps):
+        st = step(want_stats=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    paths_per_step = WIDTH * HEIGHT * SPP
+    value = paths_per_step * ws / ms * 1e-3          # Mpaths/s, whole job
+
+    # ---- per-kernel times for the roofline (live, CUDA events) ------------
+    os.environ["SNOG_PROFILE_KERNELS"] = "1"
+    prof = step(want_stats=True)
+    del os.environ["SNOG_PROFILE_KERNELS"]
+    launches = prof["kernel_launches"]
+
+    # ---- e2e through the public host API ----------------------------------
+    pinned = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, pin_memory=True)
+    host = pinned.numpy()
+    barrier()
+    t0 = time.perf_counter()
+    n_e2e = max(1, args.steps)
+    for _ in range(n_e2e):
+        cs, ps = sb.camera_struct(cam), sb.params_struct(params)
+        stt = sb.SnogRenderStats()
+        sb._check(sb._render(scene.handle, ctypes.byref(cs), ctypes.byref(ps), host.ctypes.data,
+                             ctypes.byref(stt)))
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    if pg is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = paths_per_step * ws / e2e_s * 1e-6
+    h2d = ctypes.sizeof(sb.SnogCamera) + ctypes.sizeof(sb.SnogRenderParams)
+    d2h = WIDTH * HEIGHT * 3 * 4
+
+    # ---- CPU baseline (rank 0, N=1) and algorithmic bytes ------------------
+    cpu = None
+    bytes_ray = None
+    if rank == 0:
+        ok, _ = ref_available()
+        if ok and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            recs = run_reference(sd, cam, params, 2, 1, threads)
+            r = recs[-1]
+            bytes_ray = algorithmic_bytes_per_ray(r)
+            if ws == 1:
+                cpu = {"value": round(r["mpaths_per_s"], 4), "unit": "Mpaths/s", "cores": threads,
+                       "kind": "reference",
+                       "sample": f"{WIDTH}x{HEIGHT} at 2 spp (of {SPP}), all rows, "
+                                 f"{r['seconds']:.1f} s"}
+    roofline = None
+    peaks = {}
+    pk_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        with open(pk_path) as f:
+            peaks = json.load(f)
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    if prof["closest_launches"]:
+        per_launch_ms = prof["closest_ms"] / prof["closest_launches"]
+        rays_per_launch = prof["closest_rays"] / prof["closest_launches"]
+        if bytes_ray is not None:
+            b_ray, src = bytes_ray[0], "reference traversal counts"
+        else:
+            # own counts: nodes entered and primitives tested by the kernel
+            b_ray = 36 + (36 * prof["closest_nodes"] + 40 * prof["closest_tests"]) / max(
+                prof["closest_rays"], 1)
+            src = "kernel's own traversal counts"
+        achieved = b_ray * rays_per_launch / (per_launch_ms * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": "k_trace_closest", "achieved": round(achieved, 1),
+                    "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                    "peak_source": peak_src, "bytes_per_ray": round(b_ray, 1),
+                    "bytes_source": src, "rays_per_launch": round(rays_per_launch),
+                    "ms_per_launch": round(per_launch_ms, 4), "traffic": None,
+                    "kernel_share": {k: round(prof[k + "_ms"] / max(prof["device_ms"], 1e-9), 4)
+                                     for k in ("closest", "shadow", "shade", "other")}}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 4), "unit": "Mpaths/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded terrain scene; inputs larger than L2, no flush)",
+                "config": {"workload": "terrain-2M-tris+200-spheres+sky-envmap", "width": WIDTH,
+                           "height": HEIGHT, "spp": SPP, "max_path_len": MAX_LEN,
+                           "parallelism": f"replicas x{ws}", "l2": "working set > L2"},
+                "gpu_launches": launches * args.steps,
+                "e2e": {"value": round(e2e_value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+                "rays": {"closest_per_step": prof["closest_rays"],
+                         "shadow_per_step": prof["shadow_rays"],
+                         "mrays_per_s": round((prof["closest_rays"] + prof["shadow_rays"]) * ws
+                                              / ms * 1e-3, 2)}}
+        print(json.dumps(line))
+    scene.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--width", type=int, default=WIDTH, help="smaller case for profiling only")
+    ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--spp", type=int, default=SPP)
+    args = ap.parse_args()
+    global WIDTH, HEIGHT, SPP
+    WIDTH, HEIGHT, SPP = args.width, args.height, args.spp
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return bench_reference(args)
+    return bench_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

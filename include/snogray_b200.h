@@ -133,6 +133,12 @@ typedef struct SnogRenderStats {
   double device_ms;          /* device time of the render, CUDA events */
   uint32_t waves;            /* wavefront batches the render was split into */
   uint32_t kernel_launches;
+  /* Filled only when the environment variable SNOG_PROFILE_KERNELS=1: device
+   * time of each kernel kind summed over its launches (CUDA events on the
+   * render stream), and the traversal's node visits / primitive tests. */
+  double closest_ms, shadow_ms, shade_ms, other_ms;
+  uint32_t closest_launches, shadow_launches;
+  uint64_t closest_nodes, closest_tests, shadow_nodes, shadow_tests;
 } SnogRenderStats;
 
 typedef struct SnogScene SnogScene;

@@ -14,7 +14,7 @@
 //                                   Octree::for_each_possible_intersector
 //                                   with the reference's own callbacks
 //                                   (space/space.cc:36-129)
-//   render SPEC OUT.pfm [threads] [seed_skip] [spp] [row0] [rows]
+//   render SPEC OUT.pfm [threads] [seed_skip] [spp] [row0] [rows] [repeat]
 //                                   RenderMgr::render of the whole image
 //                                   (render-mgr/render-mgr.cc:50-74), or of
 //                                   a band of rows for a bounded CPU sample
@@ -350,7 +350,7 @@ int mode_trace(const std::string &spec, const std::string &rays_path, const std:
 }
 
 int mode_render(const std::string &spec, const std::string &out, unsigned threads,
-                unsigned seed_skip, unsigned spp_override, int row0, int rows) {
+                unsigned seed_skip, unsigned spp_override, int row0, int rows, unsigned repeat) {
   RefScene rs;
   snogspec::Scene peek = snogspec::load(spec);
   (void)peek;
@@ -380,27 +380,34 @@ int mode_render(const std::string &spec, const std::string &out, unsigned thread
     y0 = row0;
     nrows = rows;
   }
-  ValTable out_params;
-  ImageSampledOutput output(out, w, hgt, out_params);
-  int xm = int(output.filter_x_radius()), ym = int(output.filter_y_radius());
-  RenderPattern pattern(0 - xm, y0 - ym, int(w) + 2 * xm, nrows + 2 * ym);
-  RenderMgr mgr(*rs.grs, camera, w, hgt);
-  NullProgress prog;
-  RenderStats stats;
-  auto t0 = std::chrono::steady_clock::now();
-  mgr.render(threads, pattern, output, prog, stats);
-  double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  unsigned spp = rs.grs->num_samples;
-  double paths = double(w) * nrows * spp;
-  printf("{\"seconds\": %.6f, \"threads\": %u, \"spp\": %u, \"rows\": %d, \"paths\": %.0f, "
-         "\"mpaths_per_s\": %.6f, \"scene_intersect_calls\": %llu, \"scene_shadow_tests\": %llu, "
-         "\"mrays_per_s\": %.6f, \"node_calls\": %llu, \"shadow_node_calls\": %llu, "
-         "\"surface_tests\": %llu, \"shadow_surface_tests\": %llu}\n",
-         secs, threads, spp, nrows, paths, paths / secs * 1e-6, stats.scene_intersect_calls,
-         stats.scene_shadow_tests,
-         double(stats.scene_intersect_calls + stats.scene_shadow_tests) / secs * 1e-6,
-         stats.intersect.space_node_intersect_calls, stats.shadow.space_node_intersect_calls,
-         stats.intersect.surface_intersects_tests, stats.shadow.surface_intersects_tests);
+  // Each repetition is an independent render of the same job into a fresh
+  // output; the scene (and its octree) is built once.
+  for (unsigned rep = 0; rep < repeat; rep++) {
+    ValTable out_params;
+    ImageSampledOutput output(out, w, hgt, out_params);
+    int xm = int(output.filter_x_radius()), ym = int(output.filter_y_radius());
+    RenderPattern pattern(0 - xm, y0 - ym, int(w) + 2 * xm, nrows + 2 * ym);
+    RenderMgr mgr(*rs.grs, camera, w, hgt);
+    NullProgress prog;
+    RenderStats stats;
+    auto t0 = std::chrono::steady_clock::now();
+    mgr.render(threads, pattern, output, prog, stats);
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    unsigned spp = rs.grs->num_samples;
+    double paths = double(w) * nrows * spp;
+    printf("{\"rep\": %u, \"seconds\": %.6f, \"threads\": %u, \"spp\": %u, \"rows\": %d, \"paths\": %.0f, "
+           "\"mpaths_per_s\": %.6f, \"scene_intersect_calls\": %llu, \"scene_shadow_tests\": %llu, "
+           "\"mrays_per_s\": %.6f, \"node_calls\": %llu, \"shadow_node_calls\": %llu, "
+           "\"surface_tests\": %llu, \"shadow_surface_tests\": %llu, \"neg_cache_hits\": %llu, "
+           "\"shadow_neg_cache_hits\": %llu}\n",
+           rep, secs, threads, spp, nrows, paths, paths / secs * 1e-6, stats.scene_intersect_calls,
+           stats.scene_shadow_tests,
+           double(stats.scene_intersect_calls + stats.scene_shadow_tests) / secs * 1e-6,
+           stats.intersect.space_node_intersect_calls, stats.shadow.space_node_intersect_calls,
+           stats.intersect.surface_intersects_tests, stats.shadow.surface_intersects_tests,
+           stats.intersect.neg_cache_hits, stats.shadow.neg_cache_hits);
+    fflush(stdout);
+  }
   return 0;
 }
 
@@ -416,7 +423,8 @@ int main(int argc, char **argv) {
     if (mode == "render" && argc >= 4)
       return mode_render(argv[2], argv[3], argc > 4 ? atoi(argv[4]) : 1,
                          argc > 5 ? atoi(argv[5]) : 0, argc > 6 ? atoi(argv[6]) : 0,
-                         argc > 7 ? atoi(argv[7]) : 0, argc > 8 ? atoi(argv[8]) : 0);
+                         argc > 7 ? atoi(argv[7]) : 0, argc > 8 ? atoi(argv[8]) : 0,
+                         argc > 9 ? unsigned(atoi(argv[9])) : 1u);
     throw std::runtime_error("bad arguments");
   } catch (std::exception &e) {
     fprintf(stderr, "snog_ref: %s\n", e.what());

@@ -80,7 +80,12 @@ class SnogSceneInfo(C.Structure):
 
 class SnogRenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("device_ms", C.c_double), ("waves", C.c_uint32), ("kernel_launches", C.c_uint32)]
+                ("device_ms", C.c_double), ("waves", C.c_uint32), ("kernel_launches", C.c_uint32),
+                ("closest_ms", C.c_double), ("shadow_ms", C.c_double), ("shade_ms", C.c_double),
+                ("other_ms", C.c_double), ("closest_launches", C.c_uint32),
+                ("shadow_launches", C.c_uint32), ("closest_nodes", C.c_uint64),
+                ("closest_tests", C.c_uint64), ("shadow_nodes", C.c_uint64),
+                ("shadow_tests", C.c_uint64)]
 
 
 def _sig(name, res, *args):

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -73,11 +74,160 @@ struct DevBuf {
   T *as() const { return static_cast<T *>(p); }
 };
 
+void RenderCache::release() {
+  wave_free(wb);
+  cudaFree(accum);
+  cudaFree(wsum);
+  cudaFree(out);
+  accum = nullptr;
+  wsum = nullptr;
+  out = nullptr;
+  npix_cap = 0;
+}
+
+// Paths per wave: SNOG_WAVE_PATHS if set, else 4M, limited to what fits in
+// a quarter of the free device memory and to the job's own path count.
+static uint64_t choose_wave_cap(uint64_t total_paths, uint32_t spp, uint32_t n_lights) {
+  uint64_t cap = 1ull << 22;
+  if (const char *e = getenv("SNOG_WAVE_PATHS")) cap = strtoull(e, nullptr, 10);
+  size_t free_b = 0, tot_b = 0;
+  if (cudaMemGetInfo(&free_b, &tot_b) == cudaSuccess) {
+    uint64_t fit = (free_b / 4) / wave_bytes_per_path(n_lights);
+    if (cap > fit) cap = fit;
+  }
+  if (cap > total_paths) cap = total_paths;
+  cap = (cap / spp) * spp;
+  if (cap < spp) cap = spp;
+  return (cap + 255) & ~uint64_t(255);
+}
+
+static void check_params(const SnogRenderParams &p) {
+  if (p.width == 0 || p.height == 0 || p.spp == 0)
+    throw Error{SNOG_EINVAL, "width, height and spp must be positive"};
+  if (p.width > 65536 || p.height > 65536) throw Error{SNOG_EINVAL, "image too large"};
+  if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};
+  if (uint64_t(p.width + 4) * (p.height + 4) * p.spp >= (1ull << 40))
+    throw Error{SNOG_EINVAL, "too many paths in one job"};
+  if (uint64_t(p.width + 4) * (p.height + 4) >= (1ull << 32))
+    throw Error{SNOG_EINVAL, "render pattern too large"};
+}
+
+// Render into the scene's cached accumulator; the resolved image goes to
+// d_out (device).  Caller holds the scene lock.
+static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
+                        cudaStream_t st, SnogRenderStats *stats) {
+  check_params(p);
+  if (!stack_class_for_depth(S.dev.max_depth))
+    throw Error{SNOG_EINVAL, "octree deeper than the traversal kernels support (84 levels)"};
+  RenderCache &rc = S.rc;
+  const uint64_t total = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
+  uint64_t cap = choose_wave_cap(total, p.spp, S.dev.n_lights);
+  if (rc.wb.wave_cap < cap || rc.wb.n_lights != S.dev.n_lights) {
+    cudaError_t e = wave_alloc(rc.wb, cap, S.dev.n_lights);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{SNOG_ENOMEM, std::string("wave buffers: ") + cudaGetErrorString(e)};
+    }
+  }
+  const size_t npix = size_t(p.width) * p.height;
+  if (rc.npix_cap < npix) {
+    cudaFree(rc.accum);
+    cudaFree(rc.wsum);
+    cudaFree(rc.out);
+    rc.accum = nullptr;
+    rc.wsum = nullptr;
+    rc.out = nullptr;
+    rc.npix_cap = 0;
+    check_cuda(cudaMalloc(&rc.accum, npix * sizeof(float4)), "accum");
+    check_cuda(cudaMalloc(&rc.wsum, npix * sizeof(float)), "wsum");
+    check_cuda(cudaMalloc(&rc.out, npix * 3 * sizeof(float)), "out");
+    rc.npix_cap = npix;
+  }
+  JobConsts jc = make_job(S.dev, cam, p);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (stats) {
+    check_cuda(cudaEventCreate(&e0), "event");
+    check_cuda(cudaEventCreate(&e1), "event");
+    check_cuda(cudaEventRecord(e0, st), "event record");
+  }
+  uint32_t waves = 0, launches = 0;
+  const char *pe = getenv("SNOG_PROFILE_KERNELS");
+  const bool profile = stats && pe && pe[0] == '1';
+  RenderProfile prof;
+  cudaError_t e = render_job(S.dev, jc, rc.wb, rc.accum, rc.wsum, d_out ? d_out : rc.out, st, &waves,
+                             &launches, profile ? &prof : nullptr);
+  if (e != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    throw Error{SNOG_ECUDA, std::string("render: ") + cudaGetErrorString(e)};
+  }
+  if (stats) {
+    check_cuda(cudaEventRecord(e1, st), "event record");
+    check_cuda(cudaEventSynchronize(e1), "render sync");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    unsigned long long hs[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t flags[4] = {0, 0, 0, 0};
+    check_cuda(cudaMemcpy(hs, rc.wb.stats, 48, cudaMemcpyDeviceToHost), "stats");
+    check_cuda(cudaMemcpy(flags, rc.wb.counters, 16, cudaMemcpyDeviceToHost), "flags");
+    if (flags[3]) throw Error{SNOG_EINVAL, "traversal stack overflow (non-finite ray?)"};
+    stats->paths = total;
+    stats->closest_rays = hs[0];
+    stats->shadow_rays = hs[1];
+    stats->device_ms = ms;
+    stats->waves = waves;
+    stats->kernel_launches = launches;
+    if (profile) {
+      check_cuda(prof.collect(), "profile events");
+      stats->closest_ms = prof.ms[RenderProfile::CLOSEST];
+      stats->shadow_ms = prof.ms[RenderProfile::SHADOW];
+      stats->shade_ms = prof.ms[RenderProfile::SHADE];
+      stats->other_ms = prof.ms[RenderProfile::OTHER];
+      stats->closest_launches = prof.launches[RenderProfile::CLOSEST];
+      stats->shadow_launches = prof.launches[RenderProfile::SHADOW];
+      stats->closest_nodes = hs[2];
+      stats->closest_tests = hs[3];
+      stats->shadow_nodes = hs[4];
+      stats->shadow_tests = hs[5];
+    }
+  }
+}
+
 }  // namespace snog
 
 using namespace snog;
 
 extern "C" {
+
+int snog_render(SnogScene *scene, const SnogCamera *camera, const SnogRenderParams *params, float *out_rgb,
+                SnogRenderStats *stats) {
+  return guarded([&] {
+    if (!scene || !camera || !params || !out_rgb) throw Error{SNOG_EINVAL, "null argument"};
+    SceneImpl &S = *scene->impl;
+    if (!S.on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
+    std::lock_guard<std::mutex> lk(S.mu);
+    SnogRenderStats local{};
+    render_into(S, *camera, *params, nullptr, nullptr, stats ? stats : &local);
+    check_cuda(cudaMemcpy(out_rgb, S.rc.out, size_t(params->width) * params->height * 3 * sizeof(float),
+                          cudaMemcpyDeviceToHost),
+               "image D2H");
+    return int(SNOG_OK);
+  });
+}
+
+int snog_render_device(SnogScene *scene, const SnogCamera *camera, const SnogRenderParams *params,
+                       float *d_out_rgb, void *stream, SnogRenderStats *stats) {
+  return guarded([&] {
+    if (!scene || !camera || !params || !d_out_rgb) throw Error{SNOG_EINVAL, "null argument"};
+    SceneImpl &S = *scene->impl;
+    if (!S.on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
+    std::lock_guard<std::mutex> lk(S.mu);
+    render_into(S, *camera, *params, d_out_rgb, cudaStream_t(stream), stats);
+    return int(SNOG_OK);
+  });
+}
 
 const char *snog_version(void) { return "snogray_b200 0.1 (sm_100a)"; }
 
@@ -116,6 +266,7 @@ int snog_scene_destroy(SnogScene *scene) {
     if (!scene) return int(SNOG_OK);
     {
       std::lock_guard<std::mutex> lk(scene->impl->mu);
+      scene->impl->rc.release();
       scene->impl->arena.release();
     }
     delete scene->impl;

@@ -11,8 +11,20 @@
 #include "../../include/snogray_b200.h"
 #include "octree_build.h"
 #include "snog_common.h"
+#include "wavefront.h"
 
 namespace snog {
+
+// Device working memory of the render calls on one scene, kept between
+// calls and grown on demand.
+struct RenderCache {
+  WaveBuffers wb;
+  float4 *accum = nullptr;     // W*H colour*weight sums (+ alpha)
+  float *wsum = nullptr;       // W*H filter weight sums
+  float *out = nullptr;        // W*H*3 resolved image (host-output calls)
+  size_t npix_cap = 0;
+  void release();
+};
 
 // Device allocations owned by one scene.
 struct DeviceArena {
@@ -34,6 +46,7 @@ struct SceneImpl {
   // host copies needed by the host side of rendering
   float bbox_min[3], bbox_max[3];
   bool on_device = false;
+  RenderCache rc;
 };
 
 // Build and upload; throws snog::Error on failure.

@@ -1,0 +1,702 @@
+// wavefront.cu -- the path integrator (render/path-integ.cc:134-407) as a
+// wavefront on sm_100a.
+//
+// A job's render pattern (the image plus the Mitchell filter's 2-pixel
+// margin, snogray.lua:543-550) times its samples per pixel is processed in
+// waves of whole pixels.  Per wave:
+//   k_camera                 eye rays for every path (camera/camera.cc:108-160)
+//   per bounce b = 0..max_len:
+//     k_trace_closest        octree closest hit for the live rays
+//     k_shade                emission, direct lighting with MIS (emits
+//                            shadow rays), BSDF continuation, Russian
+//                            roulette; appends surviving rays to the other
+//                            queue with warp-aggregated atomics
+//     k_trace_shadow         any-hit for the shadow rays; unoccluded ones add
+//                            their contribution to the path's radiance
+//   k_splat                  Mitchell filter gather of the wave's samples
+//                            into the image accumulator
+// and finally k_resolve divides by the filter weight
+// (image/image-sampled-output.cc:79-123).
+//
+// Path state is SoA of 16-byte records (float4 throughput+rr ratio, float4
+// radiance+alpha) plus a 32-bit word: path length (8 bits), after-specular
+// (1 bit), media-stack depth (2 bits) and up to three medium ids (7 bits
+// each).  Queues hold rays as two float4 (origin+t0, direction+t1) in queue
+// order, so the trace kernels read them with coalesced 128-bit loads.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "launch.h"
+#include "shade.cuh"
+#include "wavefront.h"
+
+namespace snog {
+
+namespace {
+
+// ---- path state word ------------------------------------------------------
+__device__ __forceinline__ uint32_t ps_len(uint32_t p) { return p & 0xffu; }
+__device__ __forceinline__ bool ps_spec(uint32_t p) { return (p >> 8) & 1u; }
+__device__ __forceinline__ uint32_t ps_depth(uint32_t p) { return (p >> 9) & 3u; }
+__device__ __forceinline__ uint32_t ps_medium(uint32_t p, uint32_t k) { return (p >> (11 + 7 * k)) & 0x7fu; }
+
+// Media::update_stack_for_transmission (material/media.cc:76-118): entering a
+// surface with a medium pushes it, leaving pops (never below the camera's
+// medium).  The stack holds three entries; a fourth push drops the oldest.
+__device__ __forceinline__ uint32_t ps_push(uint32_t p, uint32_t mid) {
+  uint32_t d = ps_depth(p);
+  uint32_t ids[3] = {ps_medium(p, 0), ps_medium(p, 1), ps_medium(p, 2)};
+  if (d == 3) {
+    ids[0] = ids[1];
+    ids[1] = ids[2];
+    d = 2;
+  }
+  ids[d] = mid & 0x7fu;
+  d++;
+  return (p & 0x1ffu) | (d << 9) | (ids[0] << 11) | (ids[1] << 18) | (ids[2] << 25);
+}
+__device__ __forceinline__ uint32_t ps_pop(uint32_t p) {
+  uint32_t d = ps_depth(p);
+  if (d == 0) return p;
+  return (p & ~(3u << 9)) | ((d - 1) << 9);
+}
+
+struct PathPtrs {
+  float4 *thr, *rad;
+  uint32_t *pstate;
+  float2 *jit;
+};
+struct RayQ {
+  float4 *o, *d;
+  uint32_t *path;
+};
+struct ShadowQ {
+  float4 *o, *d, *c;
+};
+
+// RNG dimensions: vertex b, slot k.
+enum : uint32_t { K_CAMERA = 0, K_BSDF = 1, K_RR = 2, K_LIGHT0 = 3 };
+__device__ __forceinline__ uint32_t dim_of(uint32_t b, uint32_t k) { return (b << 12) | k; }
+
+__device__ __forceinline__ Strata strata_for(uint32_t n) {
+  // Grid::adjust_uv_sample_count (render/grid.cc:70-80)
+  double sq = sqrt(double(n));
+  uint32_t up = uint32_t(ceil(sq)), down = uint32_t(floor(sq + 0.5));
+  if (down == 0) down = 1;
+  return Strata{n, up, down, up * down};
+}
+
+__device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred) {
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned mask = __ballot_sync(0xffffffffu, pred);
+  if (!mask) return 0;
+  uint32_t leader = __ffs(mask) - 1, base = 0;
+  if (lane == leader) base = atomicAdd(counter, uint32_t(__popc(mask)));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
+}
+
+// ---- kernels -----------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_camera(JobConsts jc, uint64_t base, uint32_t n, PathPtrs P, RayQ q,
+                                                uint32_t *counters) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[0] = n;
+    counters[1] = 0;
+    counters[2] = 0;
+  }
+  const Strata st = strata_for(jc.S);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    const uint64_t g = base + p;
+    const uint32_t pixel = uint32_t(g / jc.S), s = uint32_t(g % jc.S);
+    const int px = int(pixel % jc.PW) - 2, py = int(pixel / jc.PW) - 2;
+    Rng rng{jc.seed_lo, jc.seed_hi, uint32_t(g), uint32_t(g >> 32)};
+    float2 j = strat_uv(st, rng, pixel, s, dim_of(0, K_CAMERA));
+    // Renderer::render_packet (render-mgr/renderer.cc:69-88) and
+    // Camera::eye_vec (camera/camera.h:384-389).
+    float cu = float(px) + j.x, cv = float(py) + j.y;
+    float fu = cu / float(jc.W), fv = (float(jc.H) - cv) / float(jc.H);
+    float x = 2.f * fu - 1.f, y = 2.f * fv - 1.f;
+    float3 d = add(add(load3(jc.cam_fwd), mul(mul(load3(jc.cam_right), x), jc.tan_x)),
+                   mul(mul(load3(jc.cam_up), y), jc.tan_y));
+    q.o[p] = make_float4(jc.cam_pos[0], jc.cam_pos[1], jc.cam_pos[2], 0.f);
+    q.d[p] = make_float4(d.x, d.y, d.z, jc.max_trace);
+    q.path[p] = p;
+    P.thr[p] = make_float4(1.f, 1.f, 1.f, 1.f);
+    P.rad[p] = make_float4(0.f, 0.f, 0.f, 1.f);
+    P.pstate[p] = 0;
+    P.jit[p] = j;
+  }
+}
+
+// Add a thread's node/test counts to P[0..1] with one atomic per warp; every
+// lane of the block must call it.
+__device__ __forceinline__ void warp_count(unsigned long long *p, unsigned long long nodes,
+                                           unsigned long long tests) {
+  for (int off = 16; off > 0; off >>= 1) {
+    nodes += __shfl_down_sync(0xffffffffu, nodes, off);
+    tests += __shfl_down_sync(0xffffffffu, tests, off);
+  }
+  if ((threadIdx.x & 31u) == 0) {
+    atomicAdd(p, nodes);
+    atomicAdd(p + 1, tests);
+  }
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_trace_closest(DevScene s, RayQ q, uint32_t *counters, uint32_t cur,
+                                                       uint32_t *hit_ref, float *hit_t,
+                                                       unsigned long long *stats, bool prof) {
+  const uint32_t n = counters[cur];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counters[cur ^ 1u] = 0;   // next queue and shadow queue start empty
+    counters[2] = 0;
+    stats[0] += n;
+  }
+  unsigned long long nodes = 0, tests = 0;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    float4 o = q.o[i], d = q.d[i];
+    float t1 = d.w;
+    TraceCounters c{0, 0, 0};
+    uint32_t ref = traverse<false, STACK>(s, xyz(o), xyz(d), o.w, t1, c);
+    hit_ref[i] = ref;
+    hit_t[i] = t1;
+    if (c.overflow) atomicOr(counters + 3, 1u);
+    nodes += c.nodes;
+    tests += c.tests;
+  }
+  if (prof) warp_count(stats + 2, nodes, tests);
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) k_trace_shadow(DevScene s, ShadowQ q, uint32_t *counters, float4 *rad,
+                                                      unsigned long long *stats, bool prof) {
+  const uint32_t n = counters[2];
+  if (blockIdx.x == 0 && threadIdx.x == 0) stats[1] += n;
+  unsigned long long nodes = 0, tests = 0;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    float4 o = q.o[i], d = q.d[i];
+    float t1 = d.w;
+    TraceCounters c{0, 0, 0};
+    uint32_t ref = traverse<true, STACK>(s, xyz(o), xyz(d), o.w, t1, c);
+    if (c.overflow) atomicOr(counters + 3, 1u);
+    nodes += c.nodes;
+    tests += c.tests;
+    if (ref == PREF_END) {
+      float4 cc = q.c[i];
+      float4 *r = rad + __float_as_uint(cc.w);
+      atomicAdd(&r->x, cc.x);
+      atomicAdd(&r->y, cc.y);
+      atomicAdd(&r->z, cc.z);
+    }
+  }
+  if (prof) warp_count(stats + 4, nodes, tests);
+}
+
+__device__ __forceinline__ float3 medium_transmittance(const DevMedium &m, float len) {
+  // Medium::transmittance (material/medium.h:37-40), pow (e, -absorb * d).
+  if (m.absorb[0] == 0.f && m.absorb[1] == 0.f && m.absorb[2] == 0.f) return f3(1.f, 1.f, 1.f);
+  return f3(expf(-m.absorb[0] * len), expf(-m.absorb[1] * len), expf(-m.absorb[2] * len));
+}
+
+__global__ void __launch_bounds__(128) k_shade(DevScene s, JobConsts jc, uint64_t base, uint32_t bounce,
+                                               RayQ qin, uint32_t *counters, uint32_t cur,
+                                               const uint32_t *hit_ref, const float *hit_t, PathPtrs P,
+                                               RayQ qout, ShadowQ sq) {
+  const uint32_t n = counters[cur];
+  uint32_t *count_out = counters + (cur ^ 1u);
+  uint32_t *count_sq = counters + 2;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const Strata st = strata_for(jc.S);
+  const Strata st_direct = strata_for(jc.S * (jc.direct_samples ? jc.direct_samples : 1));
+  const Strata st_rand = strata_for(jc.direct_samples ? jc.direct_samples : 1);
+  const bool strat = bounce < jc.min_len;
+  const float inv_ns = jc.direct_samples ? 1.f / float(jc.direct_samples) : 0.f;
+
+  for (uint32_t wb = warp * 32; wb < n; wb += nwarps * 32) {
+    const uint32_t i = wb + lane;
+    const bool active = i < n;
+    uint32_t path = 0, ps = 0, ref = PREF_END;
+    float4 o4 = make_float4(0, 0, 0, 0), d4 = o4;
+    float3 thr = f3(0, 0, 0), rad = f3(0, 0, 0);
+    float rr_ratio = 1.f, alpha = 1.f;
+    bool alive = false;       // path reaches direct lighting
+    Isec I;
+    BsdfCtx B{nullptr, 1.f, 1.f};
+    DevMedium med{1.f, {0, 0, 0}};
+    Rng rng{jc.seed_lo, jc.seed_hi, 0, 0};
+    uint32_t pixel = 0, sidx = 0;
+    if (active) {
+      path = qin.path[i];
+      o4 = qin.o[i];
+      d4 = qin.d[i];
+      ref = hit_ref[i];
+      float t = hit_t[i];
+      ps = P.pstate[path];
+      float4 t4 = P.thr[path], r4 = P.rad[path];
+      thr = xyz(t4);
+      rr_ratio = t4.w;
+      rad = xyz(r4);
+      alpha = r4.w;
+      const uint64_t g = base + path;
+      pixel = uint32_t(g / jc.S);
+      sidx = uint32_t(g % jc.S);
+      rng.path_lo = uint32_t(g);
+      rng.path_hi = uint32_t(g >> 32);
+      const uint32_t depth = ps_depth(ps);
+      const uint32_t mid = depth ? ps_medium(ps, depth - 1) : 0u;
+      med = s.media[mid];
+      const uint32_t len = ps_len(ps);
+      // Volume integrator: attenuation over the ray (render/filter-volume-integ.h:55-68).
+      const float t1 = ref == PREF_END ? d4.w : t;
+      thr = mul3(thr, medium_transmittance(med, length(xyz(d4)) * (t1 - o4.w)));
+      const bool include_emitters = len == 0 || ps_spec(ps) || jc.direct_samples == 0;
+      if (ref == PREF_END) {
+        if (include_emitters) rad = add(rad, mul3(background(s, xyz(d4)), thr));
+        if (len == 0 && rad.x == 0.f && rad.y == 0.f && rad.z == 0.f) alpha = jc.bg_alpha;
+      } else {
+        I = make_isec(s, ref, xyz(o4), xyz(d4), t);
+        const DevMaterial &M = s.mats[I.mat];
+        // Glow::Le (material/glow.cc:37-40)
+        if (include_emitters && M.type == MAT_GLOW && !I.back) rad = add(rad, mul3(load3(M.color), thr));
+        const DevMaterial *bm = bsdf_material(s, I.mat);
+        if (bm) {
+          B.m = bm;
+          B.medium_ior = med.ior;
+          // Media::enclosing_medium (material/media.h:76-79)
+          B.enclosing_ior = depth >= 2 ? s.media[ps_medium(ps, depth - 2)].ior : 1.f;
+          alive = true;
+        }
+      }
+    }
+
+    // ---- direct lighting (render/direct-illum.cc:83-255) ----------------
+    // Every lane runs the same loop so that shadow-ray appends stay
+    // warp-synchronous; lanes without a live vertex append nothing.
+    if (jc.direct_samples) {
+      const uint32_t flags = B_ALL & ~B_SPECULAR;
+      for (uint32_t l = 0; l < s.n_lights; l++) {
+        const DevLight &L = s.lights[l];
+        const bool point = is_point_light(L);
+        for (uint32_t jn = 0; jn < jc.direct_samples; jn++) {
+          bool emit_l = false, emit_b = false;
+          float3 c_l = f3(0, 0, 0), c_b = f3(0, 0, 0), dir_l = c_l, dir_b = c_l;
+          float dist_l = 0.f, dist_b = 0.f;
+          if (alive) {
+            const uint32_t kl = K_LIGHT0 + 3 * l;
+            float2 pl, pb;
+            if (strat) {
+              pl = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl));
+              pb = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl + 1));
+            } else {
+              pl = strat_uv(st_rand, rng, uint32_t(rng.path_lo ^ (bounce << 24)), jn, dim_of(bounce, kl));
+              pb = strat_uv(st_rand, rng, uint32_t(rng.path_lo ^ (bounce << 24)), jn, dim_of(bounce, kl + 1));
+            }
+            const float extra = rng.u(dim_of(bounce, kl + 2) ^ (jn << 20));
+            LSample ls = light_sample(s, L, I, pl, extra);
+            if (ls.pdf > 0.f && csum(ls.val) > 0.f) {
+              float bpdf;
+              float3 bv = bsdf_eval(B, I, ls.dir, flags, bpdf);
+              if (csum(bv) > 0.f) {
+                float3 c = ls.val;
+                float slen = (ls.dist == 0.f ? jc.horizon : ls.dist) - 2.f * jc.min_trace;
+                c = mul3(c, medium_transmittance(med, slen));
+                if (!point) c = mul(c, mis_weight(ls.pdf, bpdf));
+                c = mul3(c, bv);
+                c = mul(c, fabsf(I.cos_n(ls.dir)) / ls.pdf);
+                c_l = mul(mul3(c, thr), inv_ns);
+                dir_l = ls.dir;
+                dist_l = ls.dist;
+                emit_l = true;
+              }
+            }
+            if (!point) {
+              BSample bs = bsdf_sample(B, I, pb, flags);
+              if (bs.pdf > 0.f && csum(bs.val) > 0.f) {
+                LSample lv = light_eval(s, L, I, bs.dir);
+                if (lv.pdf > 0.f && csum(lv.val) > 0.f) {
+                  float3 c = lv.val;
+                  float slen = (lv.dist == 0.f ? jc.horizon : lv.dist) - 2.f * jc.min_trace;
+                  c = mul3(c, medium_transmittance(med, slen));
+                  c = mul(c, mis_weight(bs.pdf, lv.pdf));
+                  c = mul3(c, bs.val);
+                  c = mul(c, fabsf(I.cos_n(bs.dir)) / bs.pdf);
+                  c_b = mul(mul3(c, thr), inv_ns);
+                  dir_b = bs.dir;
+                  dist_b = lv.dist;
+                  emit_b = true;
+                }
+              }
+            }
+          }
+          // Intersect::recursive_ray (dir, max_dist) (render/intersect.cc:211-218)
+          uint32_t slot = warp_append(count_sq, emit_l);
+          if (emit_l) {
+            float3 wd = I.nf.from(dir_l);
+            float t1 = (dist_l == 0.f ? jc.horizon : dist_l) - jc.min_trace;
+            sq.o[slot] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+            sq.d[slot] = make_float4(wd.x, wd.y, wd.z, t1);
+            sq.c[slot] = make_float4(c_l.x, c_l.y, c_l.z, __uint_as_float(path));
+          }
+          slot = warp_append(count_sq, emit_b);
+          if (emit_b) {
+            float3 wd = I.nf.from(dir_b);
+            float t1 = (dist_b == 0.f ? jc.horizon : dist_b) - jc.min_trace;
+            sq.o[slot] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+            sq.d[slot] = make_float4(wd.x, wd.y, wd.z, t1);
+            sq.c[slot] = make_float4(c_b.x, c_b.y, c_b.z, __uint_as_float(path));
+          }
+        }
+      }
+    }
+
+    // ---- BSDF continuation, roulette, next ray (path-integ.cc:309-403) ----
+    bool cont = false;
+    float3 next_d = f3(0, 0, 0);
+    if (alive) {
+      const uint32_t len = ps_len(ps);
+      float2 prm = strat ? strat_uv(st, rng, pixel, sidx, dim_of(bounce, K_BSDF)) : rng.uv(dim_of(bounce, K_BSDF));
+      BSample bs = bsdf_sample(B, I, prm, B_ALL);
+      if (bs.pdf != 0.f && !(bs.val.x == 0.f && bs.val.y == 0.f && bs.val.z == 0.f)) {
+        thr = mul3(thr, mul(bs.val, fabsf(I.cos_n(bs.dir)) / bs.pdf));
+        bool stop = false;
+        if (len > jc.min_len) {
+          float p = fminf(intensity(thr) * rr_ratio, 1.f);
+          if (rng.u(dim_of(bounce, K_RR)) > p) {
+            stop = true;
+          } else {
+            thr = mul(thr, 1.f / p);
+            rr_ratio *= p;
+          }
+        }
+        if (!stop && len != jc.max_len) {
+          cont = true;
+          next_d = I.nf.from(bs.dir);
+          uint32_t nps = (ps & ~0x1ffu) | (len + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
+          if (bs.flags & B_TRANSMISSIVE) {
+            uint32_t mid = s.mats[I.mat].medium_id;
+            if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
+          }
+          ps = nps;
+        }
+      }
+    }
+    uint32_t slot = warp_append(count_out, cont);
+    if (cont) {
+      // Intersect::recursive_ray (dir) (render/intersect.cc:196-202)
+      qout.o[slot] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+      qout.d[slot] = make_float4(next_d.x, next_d.y, next_d.z, jc.horizon);
+      qout.path[slot] = path;
+    }
+    if (active) {
+      P.rad[path] = make_float4(rad.x, rad.y, rad.z, alpha);
+      if (cont) {
+        P.thr[path] = make_float4(thr.x, thr.y, thr.z, rr_ratio);
+        P.pstate[path] = ps;
+      }
+    }
+  }
+}
+
+// ImageMitchellFilt::mitchell1 with B = C = 1/3, radius 2
+// (image/image-mitchell-filt.h:50-65).
+__device__ __forceinline__ float mitchell1(float x) {
+  const float b = 1.f / 3.f, c = 1.f / 3.f;
+  x = fabsf(x);
+  if (x > 2.f) return 0.f;
+  if (x > 1.f)
+    return ((-b - 6 * c) * x * x * x + (6 * b + 30 * c) * x * x + (-12 * b - 48 * c) * x + (8 * b + 24 * c)) *
+           (1.f / 6.f);
+  return ((12 - 9 * b - 6 * c) * x * x * x + (-18 + 12 * b + 6 * c) * x * x + (6 - 2 * b)) * (1.f / 6.f);
+}
+
+// Gather the wave's samples into the target pixels they reach
+// (ImageFilterConv::add_sample, image/image-filter-conv.h:109-186): every
+// sample within the filter's support of a target pixel centre adds
+// Tint * w and w, with the negative-lobe clamp (neg_clamp = -0.1).
+__global__ void __launch_bounds__(256) k_splat(JobConsts jc, uint64_t base, uint32_t n, const float4 *rad,
+                                               const float2 *jit, float4 *accum, float *wsum, int ty0,
+                                               int nrows) {
+  const uint32_t p0 = uint32_t(base / jc.S), p1 = uint32_t((base + n) / jc.S);
+  const uint32_t total = uint32_t(nrows) * jc.W;
+  const float neg_clamp = -0.1f;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int tx = int(t % jc.W), ty = ty0 + int(t / jc.W);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    float wacc = 0.f;
+    for (int dy = -2; dy <= 2; dy++) {
+      const int row = ty + dy + 2;
+      if (row < 0 || row >= int(jc.PH)) continue;
+      for (int dx = -2; dx <= 2; dx++) {
+        const int col = tx + dx + 2;
+        if (col < 0 || col >= int(jc.PW)) continue;
+        const uint32_t pidx = uint32_t(row) * jc.PW + uint32_t(col);
+        if (pidx < p0 || pidx >= p1) continue;
+        const uint32_t pbase = (pidx - p0) * jc.S;
+        for (uint32_t k = 0; k < jc.S; k++) {
+          float2 j = jit[pbase + k];
+          float sx = float(tx + dx) + j.x, sy = float(ty + dy) + j.y;
+          float w = mitchell1(sx - (float(tx) + 0.5f)) * mitchell1(sy - (float(ty) + 0.5f));
+          if (w == 0.f) continue;
+          float4 r = rad[pbase + k];
+          // Tint (radiance, alpha) stores alpha-scaled colour (color/tint.h:45-49)
+          float cr = r.x * r.w * w, cg = r.y * r.w * w, cb = r.z * r.w * w, ca = r.w * w;
+          if (w < 0.f) {
+            float mc = fminf(cr, fminf(cg, cb));
+            if (mc < neg_clamp) {
+              float sc = neg_clamp / mc;
+              w *= sc;
+              cr *= sc; cg *= sc; cb *= sc; ca *= sc;
+            }
+          }
+          acc.x += cr; acc.y += cg; acc.z += cb; acc.w += ca;
+          wacc += w;
+        }
+      }
+    }
+    const size_t o = size_t(ty) * jc.W + size_t(tx);
+    float4 a = accum[o];
+    accum[o] = make_float4(a.x + acc.x, a.y + acc.y, a.z + acc.z, a.w + acc.w);
+    wsum[o] += wacc;
+  }
+}
+
+// ImageSampledOutput::set_raw_min_y row flush (image/image-sampled-output.cc:79-123).
+__global__ void __launch_bounds__(256) k_resolve(uint32_t npix, const float4 *accum, const float *wsum, float *out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+    float4 a = accum[i];
+    float w = wsum[i];
+    float r = a.x, g = a.y, b = a.z, al = a.w;
+    if (w > 0.f && w != 1.f) {
+      float iw = 1.f / w;
+      r *= iw; g *= iw; b *= iw; al *= iw;
+    }
+    al = fminf(fmaxf(al, 0.f), 1.f);
+    r = fmaxf(r, 0.f); g = fmaxf(g, 0.f); b = fmaxf(b, 0.f);
+    if (al != 0.f && al != 1.f) {
+      float ia = 1.f / al;
+      r *= ia; g *= ia; b *= ia;
+    }
+    out[3 * size_t(i)] = r;
+    out[3 * size_t(i) + 1] = g;
+    out[3 * size_t(i) + 2] = b;
+  }
+}
+
+template <int STACK>
+void launch_bounce(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, uint64_t base, uint32_t b,
+                   uint32_t cur, uint32_t grid128, cudaStream_t st, RenderProfile *prof) {
+  RayQ qin{wb.q_o[cur], wb.q_d[cur], wb.q_path[cur]};
+  RayQ qout{wb.q_o[cur ^ 1], wb.q_d[cur ^ 1], wb.q_path[cur ^ 1]};
+  ShadowQ sq{wb.s_o, wb.s_d, wb.s_c};
+  PathPtrs P{wb.thr, wb.rad, wb.pstate, wb.jit};
+  const bool pf = prof != nullptr;
+  if (pf) prof->begin(st, RenderProfile::CLOSEST);
+  k_trace_closest<STACK><<<grid128, 128, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
+  if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADE);
+  k_shade<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, P, qout, sq);
+  if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADOW);
+  k_trace_shadow<STACK><<<grid128, 128, 0, st>>>(s, sq, wb.counters, wb.rad, wb.stats, pf);
+  if (pf) prof->end(st);
+}
+
+}  // namespace
+
+cudaError_t RenderProfile::begin(cudaStream_t st, int kind) {
+  if (n == cap) {
+    uint32_t nc = cap ? 2 * cap : 256;
+    Mark *m = new Mark[nc];
+    for (uint32_t i = 0; i < n; i++) m[i] = marks[i];
+    delete[] marks;
+    marks = m;
+    cap = nc;
+  }
+  Mark &mk = marks[n];
+  mk.kind = kind;
+  cudaError_t e = cudaEventCreate(&mk.a);
+  if (e == cudaSuccess) e = cudaEventCreate(&mk.b);
+  if (e == cudaSuccess) e = cudaEventRecord(mk.a, st);
+  return e;
+}
+
+cudaError_t RenderProfile::end(cudaStream_t st) {
+  cudaError_t e = cudaEventRecord(marks[n].b, st);
+  n++;
+  return e;
+}
+
+cudaError_t RenderProfile::collect() {
+  cudaError_t err = cudaSuccess;
+  for (uint32_t i = 0; i < n; i++) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&ms, marks[i].a, marks[i].b);
+    if (e != cudaSuccess) err = e;
+    this->ms[marks[i].kind] += ms;
+    launches[marks[i].kind]++;
+    cudaEventDestroy(marks[i].a);
+    cudaEventDestroy(marks[i].b);
+  }
+  n = 0;
+  return err;
+}
+
+RenderProfile::~RenderProfile() {
+  for (uint32_t i = 0; i < n; i++) {
+    cudaEventDestroy(marks[i].a);
+    cudaEventDestroy(marks[i].b);
+  }
+  delete[] marks;
+}
+
+uint64_t wave_bytes_per_path(uint32_t n_lights) {
+  // thr 16 + rad 16 + pstate 4 + 2 queues x 36 + hit 8 + jitter 8
+  // + shadow queue 48 per entry, 2 entries per light sample
+  return 16 + 16 + 4 + 72 + 8 + 8 + 48ull * 2 * (n_lights ? n_lights : 1);
+}
+
+cudaError_t wave_alloc(WaveBuffers &wb, uint64_t cap, uint32_t n_lights) {
+  wave_free(wb);
+  const uint64_t nl = n_lights ? n_lights : 1;
+  size_t bytes = 0;
+  auto take = [&](size_t b) {
+    size_t off = bytes;
+    bytes += (b + 255) & ~size_t(255);
+    return off;
+  };
+  size_t o_thr = take(16 * cap), o_rad = take(16 * cap), o_ps = take(4 * cap);
+  size_t o_qo0 = take(16 * cap), o_qd0 = take(16 * cap), o_qp0 = take(4 * cap);
+  size_t o_qo1 = take(16 * cap), o_qd1 = take(16 * cap), o_qp1 = take(4 * cap);
+  size_t o_href = take(4 * cap), o_ht = take(4 * cap), o_jit = take(8 * cap);
+  size_t o_so = take(16 * cap * 2 * nl), o_sd = take(16 * cap * 2 * nl), o_sc = take(16 * cap * 2 * nl);
+  size_t o_cnt = take(64), o_stats = take(64);
+  char *base = nullptr;
+  cudaError_t e = cudaMalloc(&base, bytes);
+  if (e != cudaSuccess) return e;
+  wb.block = base;
+  wb.bytes = bytes;
+  wb.wave_cap = cap;
+  wb.n_lights = n_lights;
+  wb.thr = reinterpret_cast<float4 *>(base + o_thr);
+  wb.rad = reinterpret_cast<float4 *>(base + o_rad);
+  wb.pstate = reinterpret_cast<uint32_t *>(base + o_ps);
+  wb.q_o[0] = reinterpret_cast<float4 *>(base + o_qo0);
+  wb.q_d[0] = reinterpret_cast<float4 *>(base + o_qd0);
+  wb.q_path[0] = reinterpret_cast<uint32_t *>(base + o_qp0);
+  wb.q_o[1] = reinterpret_cast<float4 *>(base + o_qo1);
+  wb.q_d[1] = reinterpret_cast<float4 *>(base + o_qd1);
+  wb.q_path[1] = reinterpret_cast<uint32_t *>(base + o_qp1);
+  wb.hit_ref = reinterpret_cast<uint32_t *>(base + o_href);
+  wb.hit_t = reinterpret_cast<float *>(base + o_ht);
+  wb.jit = reinterpret_cast<float2 *>(base + o_jit);
+  wb.s_o = reinterpret_cast<float4 *>(base + o_so);
+  wb.s_d = reinterpret_cast<float4 *>(base + o_sd);
+  wb.s_c = reinterpret_cast<float4 *>(base + o_sc);
+  wb.counters = reinterpret_cast<uint32_t *>(base + o_cnt);
+  wb.stats = reinterpret_cast<unsigned long long *>(base + o_stats);
+  return cudaSuccess;
+}
+
+void wave_free(WaveBuffers &wb) {
+  if (wb.block) cudaFree(wb.block);
+  wb = WaveBuffers{};
+}
+
+JobConsts make_job(const DevScene &s, const SnogCamera &cam, const SnogRenderParams &p) {
+  JobConsts jc;
+  std::memset(&jc, 0, sizeof jc);
+  jc.W = p.width;
+  jc.H = p.height;
+  jc.PW = p.width + 4;
+  jc.PH = p.height + 4;
+  jc.S = p.spp;
+  jc.min_len = p.min_path_len;
+  jc.max_len = p.max_path_len;
+  jc.direct_samples = p.direct_samples;
+  jc.min_trace = p.min_trace;
+  jc.bg_alpha = p.bg_alpha;
+  jc.horizon = s.horizon;
+  // (scene.bbox () + camera.pos).diameter () (render-mgr/renderer.cc:54)
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; k++) {
+    lo[k] = s.bbox_min[k] < cam.pos[k] ? s.bbox_min[k] : cam.pos[k];
+    hi[k] = s.bbox_max[k] > cam.pos[k] ? s.bbox_max[k] : cam.pos[k];
+  }
+  float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+  jc.max_trace = std::sqrt(ex * ex + ey * ey + ez * ez);
+  for (int k = 0; k < 3; k++) {
+    jc.cam_pos[k] = cam.pos[k];
+    jc.cam_fwd[k] = cam.forward[k];
+    jc.cam_right[k] = cam.right[k];
+    jc.cam_up[k] = cam.up[k];
+  }
+  jc.tan_x = cam.tan_half_fov_x;
+  jc.tan_y = cam.tan_half_fov_y;
+  jc.seed_lo = uint32_t(p.seed) * 2654435761u + 0x1234567u;
+  jc.seed_hi = uint32_t(p.seed >> 32) ^ 0x9e3779b9u;
+  return jc;
+}
+
+cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, float4 *accum, float *wsum,
+                       float *out_rgb, cudaStream_t st, uint32_t *waves, uint32_t *launches,
+                       RenderProfile *prof) {
+  const uint64_t npix = uint64_t(jc.W) * jc.H;
+  cudaError_t e = cudaMemsetAsync(accum, 0, npix * sizeof(float4), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(wsum, 0, npix * sizeof(float), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(wb.stats, 0, 64, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(wb.counters, 0, 64, st);
+  if (e != cudaSuccess) return e;
+  const int sms = num_sms();
+  const uint32_t grid128 = uint32_t(sms) * 12, grid256 = uint32_t(sms) * 8;
+  const uint64_t total = uint64_t(jc.PW) * jc.PH * jc.S;
+  const uint64_t wave_paths = (wb.wave_cap / jc.S) * jc.S;
+  if (wave_paths == 0) return cudaErrorInvalidValue;
+  const int sc = stack_class_for_depth(s.max_depth);
+  uint32_t nl = 0;
+  for (uint64_t base = 0; base < total; base += wave_paths) {
+    const uint32_t n = uint32_t(total - base < wave_paths ? total - base : wave_paths);
+    PathPtrs P{wb.thr, wb.rad, wb.pstate, wb.jit};
+    RayQ q0{wb.q_o[0], wb.q_d[0], wb.q_path[0]};
+    if (prof) prof->begin(st, RenderProfile::OTHER);
+    k_camera<<<grid256, 256, 0, st>>>(jc, base, n, P, q0, wb.counters);
+    if (prof) prof->end(st);
+    nl++;
+    for (uint32_t b = 0; b <= jc.max_len; b++) {
+      const uint32_t cur = b & 1u;
+      switch (sc) {
+        case 32: launch_bounce<32>(s, jc, wb, base, b, cur, grid128, st, prof); break;
+        case 64: launch_bounce<64>(s, jc, wb, base, b, cur, grid128, st, prof); break;
+        case 128: launch_bounce<128>(s, jc, wb, base, b, cur, grid128, st, prof); break;
+        case 256: launch_bounce<256>(s, jc, wb, base, b, cur, grid128, st, prof); break;
+        default: return cudaErrorInvalidValue;
+      }
+      nl += 3;
+    }
+    // Output rows reached by this wave's pattern rows.
+    const uint32_t p0 = uint32_t(base / jc.S), p1 = uint32_t((base + n) / jc.S);
+    int r0 = int(p0 / jc.PW), r1 = int((p1 - 1) / jc.PW);
+    int ty0 = r0 - 4 < 0 ? 0 : r0 - 4, ty1 = r1 > int(jc.H) - 1 ? int(jc.H) - 1 : r1;
+    if (ty1 >= ty0) {
+      if (prof) prof->begin(st, RenderProfile::OTHER);
+      k_splat<<<grid256, 256, 0, st>>>(jc, base, n, wb.rad, P.jit, accum, wsum, ty0, ty1 - ty0 + 1);
+      if (prof) prof->end(st);
+      nl++;
+    }
+    if (waves) (*waves)++;
+  }
+  if (prof) prof->begin(st, RenderProfile::OTHER);
+  k_resolve<<<grid256, 256, 0, st>>>(uint32_t(npix), accum, wsum, out_rgb);
+  if (prof) prof->end(st);
+  nl++;
+  if (launches) *launches += nl;
+  return cudaGetLastError();
+}
+
+}  // namespace snog

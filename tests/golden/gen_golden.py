@@ -131,13 +131,13 @@ def image_stats(imgs):
 
 
 RENDER_CASES = {
-    "cornell": (scenes.cornell_box, scenes.cornell_camera, scenes.cornell_params, 64, 64, 16),
+    "cornell": (scenes.cornell_box, scenes.cornell_camera, scenes.cornell_params, 128, 128, 16),
     "terrain": (lambda: scenes.terrain_scene(n=96, n_spheres=40, seed=11, env_w=256, env_h=128),
                 scenes.terrain_camera, scenes.terrain_params, 64, 48, 16),
 }
 
 
-def gen_render(name, k=16, gt_spp=4096):
+def gen_render(name, k=64, gt_spp=4096):
     make_scene, make_cam, make_params, w, h, spp = RENDER_CASES[name]
     sd = make_scene()
     cam = make_cam(w, h)

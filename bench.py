@@ -184,6 +184,46 @@ def bench_reference(args):
     return 0
 
 
+def bench_isec(args, n_tri=1 << 20, n_rays=1 << 24):
+    """Intersection-only batch: 1M random triangles (centroids U[0,1]^3, edges
+    U(0.002, 0.02), random orientation), 16M rays (origins U[-0.1,1.1]^3,
+    directions uniform on the sphere, t_max = inf), half closest-hit, half
+    any-hit.  Returns a dict (Mrays/s, per-launch ms, roofline)."""
+    import torch
+    import snogray_b200 as sb
+    from snogray_b200 import scenes
+    n_rays = args.isec_rays or n_rays
+    sd = scenes.random_triangles(n_tri, seed=2)
+    sc = sb.Scene(sd)
+    rays = torch.from_numpy(scenes.random_rays(n_rays, seed=3)).cuda()
+    prim = torch.empty(n_rays, dtype=torch.int32, device="cuda")
+    tt = torch.empty(n_rays, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    nc = n_rays // 2
+    for _ in range(3):
+        sc.trace_device(rays.data_ptr(), n_rays, nc, prim.data_ptr(), tt.data_ptr(), None,
+                        stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record(stream)
+    for _ in range(reps):
+        sc.trace_device(rays.data_ptr(), n_rays, nc, prim.data_ptr(), tt.data_ptr(), None,
+                        stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    sample = rays[:, :65536].cpu().numpy()
+    _, _, _, cnt = sc.trace(sample, 32768)
+    out = {"workload": f"{n_tri} random triangles, {n_rays} rays (half closest, half any)",
+           "mrays_per_s": round(n_rays / ms * 1e-3, 2), "ms_per_launch": round(ms, 3),
+           "hit_rate_closest": round(float((prim[:nc] >= 0).float().mean()), 4),
+           "nodes_per_ray": round((cnt["closest_nodes"] + cnt["any_nodes"]) / 65536, 2),
+           "tests_per_ray": round((cnt["closest_tests"] + cnt["any_tests"]) / 65536, 2)}
+    sc.close()
+    return out
+
+
 def bench_ours(args):
     import ctypes
 
@@ -333,6 +373,7 @@ def bench_ours(args):
 
 
 def main():
+    global WIDTH, HEIGHT, SPP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -342,13 +383,20 @@ def main():
     ap.add_argument("--width", type=int, default=WIDTH, help="smaller case for profiling only")
     ap.add_argument("--height", type=int, default=HEIGHT)
     ap.add_argument("--spp", type=int, default=SPP)
+    ap.add_argument("--isec-only", action="store_true",
+                    help="only the intersection-only batch (1M triangles, 16M rays)")
+    ap.add_argument("--isec-rays", type=int, default=0)
     args = ap.parse_args()
-    global WIDTH, HEIGHT, SPP
     WIDTH, HEIGHT, SPP = args.width, args.height, args.spp
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return bench_reference(args)
+    if args.isec_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"isec": bench_isec(args)}))
+        return 0
     return bench_ours(args)
 
 

@@ -41,6 +41,17 @@ int num_sms() {
   return cached[dev];
 }
 
+int blocks_per_sm_cached(const void *kernel, int threads, int (*query)(const void *, int)) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<const void *, int>, int>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto &e : cache)
+    if (e.first.first == kernel && e.first.second == threads) return e.second;
+  int v = query(kernel, threads);
+  cache.push_back({{kernel, threads}, v});
+  return v;
+}
+
 template <class F>
 int guarded(F &&f) {
   try {
@@ -76,6 +87,8 @@ struct DevBuf {
 
 void RenderCache::release() {
   wave_free(wb);
+  cudaFree(trace_scratch);
+  trace_scratch = nullptr;
   cudaFree(accum);
   cudaFree(wsum);
   cudaFree(out);
@@ -293,13 +306,7 @@ int snog_scene_octree(const SnogScene *scene, uint32_t *children, uint32_t *head
     if (plist) {
       for (size_t i = 0; i < o.plist.size(); i++) {
         uint32_t r = o.plist[i];
-        if (r == PREF_END) {
-          plist[i] = -1;
-          continue;
-        }
-        uint32_t kind = r >> 30, idx = r & PREF_INDEX_MASK;
-        plist[i] = int32_t(kind == PK_TRI ? idx : kind == PK_SPHERE ? S.n_tri + idx
-                                                                     : S.n_tri + S.n_sph + idx);
+        plist[i] = r == PREF_END ? -1 : int32_t(r);
       }
     }
     return int(SNOG_OK);
@@ -316,8 +323,10 @@ int snog_trace_device(SnogScene *scene, const float *d_rays, uint32_t n, uint32_
     if (!stack_class_for_depth(S.dev.max_depth))
       throw Error{SNOG_EINVAL, "octree deeper than the traversal kernels support (84 levels)"};
     std::lock_guard<std::mutex> lk(S.mu);
+    if (!S.rc.trace_scratch) check_cuda(cudaMalloc(&S.rc.trace_scratch, 64), "trace scratch");
+    check_cuda(cudaMemsetAsync(S.rc.trace_scratch, 0, 64, cudaStream_t(stream)), "memset");
     check_cuda(launch_trace_batch(S.dev, d_rays, n, n_closest, d_prim, d_t, d_normal, nullptr,
-                                  nullptr, cudaStream_t(stream), nullptr),
+                                  S.rc.trace_scratch + 1, S.rc.trace_scratch, cudaStream_t(stream), nullptr),
                "trace launch");
     return int(SNOG_OK);
   });
@@ -343,8 +352,8 @@ int snog_trace(SnogScene *scene, const float *rays, uint32_t n, uint32_t n_close
     check_cuda(cudaMemset(d_cnt.p, 0, 64), "memset");
     check_cuda(launch_trace_batch(S.dev, d_rays.as<float>(), n, n_closest, d_prim.as<int32_t>(),
                                   t ? d_t.as<float>() : nullptr, normal ? d_nrm.as<float>() : nullptr,
-                                  d_cnt.as<unsigned long long>(), d_cnt.as<uint32_t>() + 8, nullptr,
-                                  nullptr),
+                                  d_cnt.as<unsigned long long>(), d_cnt.as<uint32_t>() + 8,
+                                  d_cnt.as<uint32_t>() + 9, nullptr, nullptr),
                "trace launch");
     check_cuda(cudaMemcpy(prim, d_prim.p, size_t(n) * 4, cudaMemcpyDeviceToHost), "prim D2H");
     if (t) check_cuda(cudaMemcpy(t, d_t.p, size_t(n) * 4, cudaMemcpyDeviceToHost), "t D2H");

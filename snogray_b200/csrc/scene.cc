@@ -103,6 +103,45 @@ Box3 box_of_points(std::initializer_list<V3> pts) {
 
 void fail(const std::string &m) { throw Error{SNOG_EINVAL, m}; }
 
+// The 16-byte device node (snog_common.h): breadth-first numbering gives the
+// children of a node consecutive ids in octant order, checked here.  The
+// surface lists are copied to PLIST4 with every list starting at a multiple
+// of 4 entries and padded with PREF_END to one.
+std::vector<uint4> compact_nodes(const OctreeArrays &o, std::vector<uint32_t> &plist4) {
+  const size_t n = o.heads.size();
+  std::vector<uint4> out(n);
+  plist4.assign(4, PREF_END);
+  for (size_t i = 0; i < n; i++) {
+    const uint32_t *k = &o.children[8 * i];
+    uint4 r{0, 0, o.heads[i], 0};
+    const bool leaf = k[0] == 1 && k[1] == 1;
+    if (!leaf) {
+      uint32_t expect = 0;
+      for (uint32_t s = 0; s < 8; s++) {
+        if (!k[s]) continue;
+        if (r.y == 0) {
+          r.x = k[s];
+          expect = k[s];
+        }
+        if (k[s] != expect) throw Error{SNOG_EINVAL, "octree children not consecutive"};
+        expect++;
+        r.y |= 1u << s;
+      }
+    }
+    if (r.z) {
+      const uint32_t start = uint32_t(plist4.size());
+      for (uint32_t e = r.z; o.plist[e] != PREF_END; e++) {
+        plist4.push_back(o.plist[e]);
+        r.w++;
+      }
+      while (plist4.size() % 4) plist4.push_back(PREF_END);
+      r.z = start;
+    }
+    out[i] = r;
+  }
+  return out;
+}
+
 template <class T>
 T *dev_upload(DeviceArena &a, const std::vector<T> &v) {
   return static_cast<T *>(a.upload(v.data(), v.size() * sizeof(T)));
@@ -139,8 +178,8 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
       fail("envmap must be a lat-long image with width == 2 * height");
   }
   if (d.n_triangles + d.n_spheres + d.n_tripars == 0) fail("scene has no surfaces");
-  if (d.n_triangles >= (1u << 30) || d.n_spheres >= (1u << 30) || d.n_tripars >= (1u << 30))
-    fail("too many primitives of one kind (limit 2^30)");
+  if (uint64_t(d.n_triangles) + d.n_spheres + d.n_tripars >= (1ull << 31))
+    fail("too many primitives (limit 2^31)");
 
   std::unique_ptr<SceneImpl> sc(new SceneImpl);
   if (upload) check_cuda(cudaGetDevice(&sc->device), "cudaGetDevice");
@@ -180,8 +219,18 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
   }
 
   // ---- primitives, bounding boxes, octree -------------------------------
+  // One 48-byte record per primitive, indexed by primitive id; the octree
+  // lists hold those ids (snog_common.h).
   BoxAcc scene_box, mesh_box;
-  std::vector<float4> tri(3 * size_t(d.n_triangles));
+  const size_t n_prims = size_t(d.n_triangles) + d.n_spheres + d.n_tripars;
+  std::vector<float4> prims(3 * n_prims, make_float4(0.f, 0.f, 0.f, 0.f));
+  std::vector<uint32_t> prim_mat(n_prims);
+  auto put = [&](size_t id, float4 a, float4 b, float4 c, uint32_t mat) {
+    prims[3 * id] = a;
+    prims[3 * id + 1] = b;
+    prims[3 * id + 2] = c;
+    prim_mat[id] = mat;
+  };
   OctreeBuilder ob;
   for (uint32_t v = 0; v < d.n_vertices; v++) mesh_box.add(v3(d.vertices + 3 * size_t(v)));
   for (uint32_t t = 0; t < d.n_triangles; t++) {
@@ -189,43 +238,37 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
     V3 p0 = v3(d.vertices + 3 * size_t(ix[0])), p1 = v3(d.vertices + 3 * size_t(ix[1])),
        p2 = v3(d.vertices + 3 * size_t(ix[2]));
     V3 e1 = vsub(p1, p0), e2 = vsub(p2, p0);
-    tri[3 * size_t(t)] = make_float4(p0.x, p0.y, p0.z, 0.f);
-    tri[3 * size_t(t) + 1] = make_float4(e1.x, e1.y, e1.z, 0.f);
-    tri[3 * size_t(t) + 2] = make_float4(e2.x, e2.y, e2.z, 0.f);
+    put(t, make_float4(p0.x, p0.y, p0.z, float(PRIM_TRI)), make_float4(e1.x, e1.y, e1.z, 0.f),
+        make_float4(e2.x, e2.y, e2.z, 0.f), d.tri_material[t]);
     // Degenerate triangles are left out of the space (surface/mesh.cc:833-846);
     // the mesh is left-handed, normal = e2 x e1 (surface/mesh.h:55).
-    if (vlen2(vcross(e2, e1)) > 0) ob.add((PK_TRI << 30) | t, box_of_points({p0, p1, p2}));
+    if (vlen2(vcross(e2, e1)) > 0) ob.add(t, box_of_points({p0, p1, p2}));
   }
   if (d.n_triangles) scene_box.add(Box3{{mesh_box.lo[0], mesh_box.lo[1], mesh_box.lo[2]},
                                        {mesh_box.hi[0], mesh_box.hi[1], mesh_box.hi[2]}});
-  std::vector<float4> sph(d.n_spheres);
-  std::vector<uint32_t> sph_mat(d.n_spheres);
   for (uint32_t i = 0; i < d.n_spheres; i++) {
     const SnogSphere &s = d.spheres[i];
-    sph[i] = make_float4(s.center[0], s.center[1], s.center[2], s.radius);
-    sph_mat[i] = s.material;
+    const uint32_t id = d.n_triangles + i;
+    put(id, make_float4(s.center[0], s.center[1], s.center[2], float(PRIM_SPHERE)),
+        make_float4(s.radius, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), s.material);
     float r = s.radius;
     Box3 b{{s.center[0] - r, s.center[1] - r, s.center[2] - r},
            {s.center[0] + r, s.center[1] + r, s.center[2] + r}};   // surface/sphere.cc:164-170
     scene_box.add(b);
-    ob.add((PK_SPHERE << 30) | i, b);
+    ob.add(id, b);
   }
-  std::vector<float4> tpar(3 * size_t(d.n_tripars));
-  std::vector<uint32_t> tpar_mat(d.n_tripars);
   for (uint32_t i = 0; i < d.n_tripars; i++) {
     const SnogTripar &p = d.tripars[i];
+    const uint32_t id = d.n_triangles + d.n_spheres + i;
     V3 v0 = v3(p.v0), e1 = v3(p.e1), e2 = v3(p.e2);
-    tpar[3 * size_t(i)] = make_float4(v0.x, v0.y, v0.z, p.parallelogram ? 1.f : 0.f);
-    tpar[3 * size_t(i) + 1] = make_float4(e1.x, e1.y, e1.z, 0.f);
-    tpar[3 * size_t(i) + 2] = make_float4(e2.x, e2.y, e2.z, 0.f);
-    tpar_mat[i] = p.material;
+    put(id, make_float4(v0.x, v0.y, v0.z, float(p.parallelogram ? PRIM_PARALLELOGRAM : PRIM_TRIPAR)),
+        make_float4(e1.x, e1.y, e1.z, 0.f), make_float4(e2.x, e2.y, e2.z, 0.f), p.material);
     Box3 b = p.parallelogram ? box_of_points({v0, vadd(v0, e1), vadd(v0, e2), vadd(vadd(v0, e1), e2)})
                              : box_of_points({v0, vadd(v0, e1), vadd(v0, e2)});   // surface/tripar.cc:188-197
     scene_box.add(b);
-    ob.add((PK_TRIPAR << 30) | i, b);
+    ob.add(id, b);
   }
   S.oct = ob.finish();
-  std::vector<uint32_t> tri_mat(d.tri_material, d.tri_material + d.n_triangles);
 
   // ---- light samplers, in the reference's order -------------------------
   std::vector<DevLight> lights;
@@ -367,15 +410,12 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
   std::memset(&D, 0, sizeof(D));
   DeviceArena &A = S.arena;
   if (upload) try {
-    D.node_children = dev_upload(A, S.oct.children);
-    D.node_heads = dev_upload(A, S.oct.heads);
-    D.plist = dev_upload(A, S.oct.plist);
-    D.tri = dev_upload(A, tri);
-    D.tri_mat = dev_upload(A, tri_mat);
-    D.sph = dev_upload(A, sph);
-    D.sph_mat = dev_upload(A, sph_mat);
-    D.tpar = dev_upload(A, tpar);
-    D.tpar_mat = dev_upload(A, tpar_mat);
+    std::vector<uint32_t> plist4;
+    std::vector<uint4> nodes = compact_nodes(S.oct, plist4);
+    D.nodes = dev_upload(A, nodes);
+    D.plist = dev_upload(A, plist4);
+    D.prims = dev_upload(A, prims);
+    D.prim_mat = dev_upload(A, prim_mat);
     D.mats = dev_upload(A, mats);
     D.lights = dev_upload(A, lights);
     D.media = dev_upload(A, media);

@@ -23,6 +23,7 @@ struct RenderCache {
   float *wsum = nullptr;       // W*H filter weight sums
   float *out = nullptr;        // W*H*3 resolved image (host-output calls)
   size_t npix_cap = 0;
+  uint32_t *trace_scratch = nullptr;   // ray-batch dispenser counter (+ flags)
   void release();
 };
 

@@ -152,28 +152,22 @@ __device__ __forceinline__ Frame3 tri_frame(const DevScene &s, float3 pos, float
 __device__ __forceinline__ Isec make_isec(const DevScene &s, uint32_t ref, float3 o, float3 d, float t) {
   Isec I;
   I.pos = add(o, mul(d, t));
-  const uint32_t kind = ref >> 30, idx = ref & PREF_INDEX_MASK;
+  const PrimRec r = load_prim(s, ref);
+  I.mat = __ldg(s.prim_mat + ref);
   Frame3 f;
-  if (kind == PK_TRI) {
-    const float4 *p = s.tri + 3 * size_t(idx);
-    float3 e1 = xyz(__ldg(p + 1)), e2 = xyz(__ldg(p + 2));
-    f = tri_frame(s, I.pos, unit(cross(e2, e1)));
-    I.mat = __ldg(s.tri_mat + idx);
-  } else if (kind == PK_SPHERE) {
-    float4 sp = __ldg(s.sph + idx);
-    float3 n = unit(sub(I.pos, xyz(sp)));
+  if (r.a.w == float(PRIM_TRI)) {
+    f = tri_frame(s, I.pos, unit(cross(xyz(r.c), xyz(r.b))));
+  } else if (r.a.w == float(PRIM_SPHERE)) {
+    float3 n = unit(sub(I.pos, xyz(r.a)));
     float3 tt = cross(n, f3(0.f, 0.f, 1.f));
     if (length_sq(tt) < 1e-15f) tt = perpendicular(n);
     tt = unit(tt);
     f = Frame3{tt, cross(tt, n), n};
-    I.mat = __ldg(s.sph_mat + idx);
   } else {
-    const float4 *p = s.tpar + 3 * size_t(idx);
-    float3 e1 = xyz(__ldg(p + 1)), e2 = xyz(__ldg(p + 2));
+    float3 e1 = xyz(r.b), e2 = xyz(r.c);
     float3 n = unit(cross(e2, e1));
     float3 sx = mul(e1, 1.0f / length(e1));
     f = Frame3{sx, cross(sx, n), n};
-    I.mat = __ldg(s.tpar_mat + idx);
   }
   // normal frame == geometric frame (no vertex normals, no bump maps)
   float3 wv = neg(unit(d));

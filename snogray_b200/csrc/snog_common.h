@@ -3,24 +3,22 @@
 // the small float3 helpers both sides use.
 //
 // Layout of one scene in device memory (all arrays 16-byte aligned):
-//   node_children  uint32[8 * n_nodes]   8 child indices per octree node, BFS
-//                                         order, 0 = none; a leaf has
-//                                         children[0] == children[1] == 1
-//                                         (space/octree-node.h:47-58)
-//   node_heads     uint32[n_nodes]        first entry of the node's surface
-//                                         list in plist, 0 = empty list
-//   plist          uint32[n_plist]        packed surface lists; an entry is
-//                                         (kind << 30 | index), PREF_END ends
-//                                         a list; plist[0] is a reserved end
-//   tri            float4[3 * n_tri]      corner, edge1, edge2 per triangle
-//                                         (edges precomputed on the host with
-//                                         the same IEEE subtraction the
-//                                         reference does per test,
-//                                         surface/mesh.cc:735-736)
-//   sph            float4[n_sph]          centre xyz, radius w
-//   tpar           float4[3 * n_tpar]     corner, edge1, edge2; corner.w = 1
-//                                         for a parallelogram, 0 for triangle
-//   *_mat          uint32[n]              material index per primitive
+//   nodes          uint4[n_nodes]         BFS order: first child, child mask,
+//                                         list start, list length (below)
+//   plist          uint32[n_plist]        surface lists of primitive ids; each
+//                                         list starts at a multiple of 4 and
+//                                         is padded with PREF_END to one, so
+//                                         4 ids come with one 128-bit load
+//   prims          float4[3 * n_prims]    one 48-byte record per primitive,
+//                                         indexed by primitive id (triangles,
+//                                         then spheres, then tripars):
+//                     triangle  a = corner, b = edge1, c = edge2 (edges
+//                               precomputed with the same IEEE subtraction the
+//                               reference does per test, surface/mesh.cc:735-736)
+//                     sphere    a = centre, b.x = radius
+//                     tripar    a = corner, b = edge1, c = edge2
+//                               a.w holds the kind (PRIM_* below, as a float)
+//   prim_mat       uint32[n_prims]        material index per primitive
 //   mats, lights, envmap texels and Hist2dDist cumulative sums
 
 #ifndef SNOG_COMMON_H
@@ -39,10 +37,10 @@
 
 namespace snog {
 
-// Primitive kinds in a packed surface-list entry.
-enum : uint32_t { PK_TRI = 0, PK_SPHERE = 1, PK_TRIPAR = 2 };
-constexpr uint32_t PREF_END = 0xffffffffu;
-constexpr uint32_t PREF_INDEX_MASK = 0x3fffffffu;
+// Primitive kinds, stored in the w component of a primitive record's first
+// float4.
+enum : uint32_t { PRIM_TRI = 0, PRIM_SPHERE = 1, PRIM_TRIPAR = 2, PRIM_PARALLELOGRAM = 3 };
+constexpr uint32_t PREF_END = 0xffffffffu;   // ends a surface list
 
 // Material kinds (same numbering as SnogMaterial::type in the C ABI).
 enum : uint32_t { MAT_LAMBERT = 0, MAT_COOK_TORRANCE = 1, MAT_MIRROR = 2, MAT_GLASS = 3, MAT_GLOW = 4 };
@@ -81,16 +79,18 @@ struct DevMedium {
   float absorb[3];
 };
 
+// One octree node in the device layout, 16 bytes (one 128-bit load).
+// Breadth-first numbering gives a node's children consecutive ids in octant
+// order, so the eight child ids of the reference's node
+// (space/octree-node.h:27-86) reduce to the first child's id and an 8-bit
+// mask: child(slot) = first + popc(mask & ((1 << slot) - 1)).
+//   x = first child id, y = child mask (0 = leaf),
+//   z = first entry of the surface list in plist, w = list length
 struct DevScene {
-  const uint32_t *node_children;
-  const uint32_t *node_heads;
+  const uint4 *nodes;
   const uint32_t *plist;
-  const float4 *tri;
-  const uint32_t *tri_mat;
-  const float4 *sph;
-  const uint32_t *sph_mat;
-  const float4 *tpar;
-  const uint32_t *tpar_mat;
+  const float4 *prims;
+  const uint32_t *prim_mat;
   const DevMaterial *mats;
   const DevLight *lights;
   const DevMedium *media;

@@ -17,34 +17,44 @@ __global__ void __launch_bounds__(128) k_trace_batch(DevScene s, const float *__
                                                      int32_t *__restrict__ prim, float *__restrict__ tout,
                                                      float *__restrict__ nrm,
                                                      unsigned long long *__restrict__ counters,
-                                                     uint32_t *__restrict__ err) {
-  const uint32_t stride = gridDim.x * blockDim.x;
+                                                     uint32_t *__restrict__ err, uint32_t *__restrict__ fetch) {
   unsigned long long cn = 0, ct = 0, an = 0, at = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    float3 o = f3(rays[i], rays[size_t(n) + i], rays[2 * size_t(n) + i]);
-    float3 d = f3(rays[3 * size_t(n) + i], rays[4 * size_t(n) + i], rays[5 * size_t(n) + i]);
-    float t1 = rays[6 * size_t(n) + i];
-    TraceCounters c{0, 0, 0};
-    const bool closest = i < n_closest;
-    uint32_t ref = closest ? traverse<false, STACK>(s, o, d, 0.f, t1, c)
-                           : traverse<true, STACK>(s, o, d, 0.f, t1, c);
+  Traversal<STACK> tr;
+  RayDispenser disp;
+  uint32_t ray = RayDispenser::kIdle;
+  TraceCounters c{0, 0, 0};
+  for (;;) {
+    bool all_idle;
+    const uint32_t got = disp.fetch(fetch, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
+    if (all_idle) break;
+    if (got != RayDispenser::kIdle) {
+      ray = got;
+      tr.init(s, f3(rays[ray], rays[size_t(n) + ray], rays[2 * size_t(n) + ray]),
+              f3(rays[3 * size_t(n) + ray], rays[4 * size_t(n) + ray], rays[5 * size_t(n) + ray]), 0.f,
+              rays[6 * size_t(n) + ray]);
+      c = TraceCounters{0, 0, 0};
+    }
+    if (ray == RayDispenser::kIdle) continue;
+    const bool closest = ray < n_closest;
+    const bool fin = closest ? tr.template step<false>(s, c) : tr.template step<true>(s, c);
+    if (!fin) continue;
+    const uint32_t i = ray, ref = tr.hit_ref;
+    ray = RayDispenser::kIdle;
     prim[i] = prim_id_of(s, ref);
-    if (tout) tout[i] = (closest && ref != PREF_END) ? t1 : 0.f;
+    if (tout) tout[i] = (closest && ref != PREF_END) ? tr.t1 : 0.f;
     if (nrm) {
       float3 nv = f3(0.f, 0.f, 0.f);
       if (closest && ref != PREF_END) {
-        const uint32_t kind = ref >> 30, idx = ref & PREF_INDEX_MASK;
-        if (kind == PK_SPHERE) {
+        const PrimRec r = load_prim(s, ref);
+        if (r.a.w == float(PRIM_SPHERE)) {
           // Sphere::IsecInfo::normal: (ray.end () - centre).unit () (surface/sphere.cc:96-100)
-          float4 sp = s.sph[idx];
-          float3 end = xadd(o, xmul(d, t1));
-          float3 v = xsub(end, xyz(sp));
+          float3 end = xadd(tr.o, xmul(tr.d, tr.t1));
+          float3 v = xsub(end, xyz(r.a));
           nv = xmul(v, __fdiv_rn(1.0f, __fsqrt_rn(xlen_sq(v))));
         } else {
           // Triangles (left-handed mesh) and tripars: (e2 x e1).unit ()
           // (surface/mesh.cc:713-718, surface/tripar.cc:78-82).
-          const float4 *p = (kind == PK_TRI ? s.tri : s.tpar) + 3 * size_t(idx);
-          float3 v = xcross(xyz(p[2]), xyz(p[1]));
+          float3 v = xcross(xyz(r.c), xyz(r.b));
           nv = xmul(v, __fdiv_rn(1.0f, __fsqrt_rn(xlen_sq(v))));
         }
       }
@@ -91,18 +101,16 @@ int stack_class_for_depth(uint32_t depth) {
 
 cudaError_t launch_trace_batch(const DevScene &s, const float *rays, uint32_t n, uint32_t n_closest,
                                int32_t *prim, float *t, float *nrm, unsigned long long *counters,
-                               uint32_t *err, cudaStream_t st, int *launches) {
+                               uint32_t *err, uint32_t *fetch, cudaStream_t st, int *launches) {
   if (n == 0) return cudaSuccess;
   const int threads = 128;
-  int sms = num_sms();
-  uint32_t blocks = (n + threads - 1) / threads;
-  uint32_t cap = uint32_t(sms) * 16;
-  if (blocks > cap) blocks = cap;
+  const uint32_t want = (n + threads - 1) / threads;
+  auto grid = [&](uint32_t resident) { return want < resident ? want : resident; };
   switch (stack_class_for_depth(s.max_depth)) {
-    case 32: k_trace_batch<32><<<blocks, threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err); break;
-    case 64: k_trace_batch<64><<<blocks, threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err); break;
-    case 128: k_trace_batch<128><<<blocks, threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err); break;
-    case 256: k_trace_batch<256><<<blocks, threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err); break;
+    case 32: k_trace_batch<32><<<grid(resident_grid(k_trace_batch<32>, threads)), threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err, fetch); break;
+    case 64: k_trace_batch<64><<<grid(resident_grid(k_trace_batch<64>, threads)), threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err, fetch); break;
+    case 128: k_trace_batch<128><<<grid(resident_grid(k_trace_batch<128>, threads)), threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err, fetch); break;
+    case 256: k_trace_batch<256><<<grid(resident_grid(k_trace_batch<256>, threads)), threads, 0, st>>>(s, rays, n, n_closest, prim, t, nrm, counters, err, fetch); break;
     default: return cudaErrorInvalidValue;
   }
   if (launches) (*launches)++;

@@ -137,32 +137,32 @@ __device__ __forceinline__ uint32_t pick_child(uint4 k0, uint4 k1, uint32_t idx)
   return (idx & 2u) ? b : a;
 }
 
-// Test the packed surface reference REF against the ray.  Closest queries
-// shrink t1 on a hit.
-__device__ __forceinline__ bool test_ref(const DevScene &s, uint32_t ref, float3 o, float3 d,
-                                         float t0, float &t1) {
-  const uint32_t kind = ref >> 30, idx = ref & PREF_INDEX_MASK;
+// A primitive's 48-byte record (snog_common.h).
+struct PrimRec {
+  float4 a, b, c;
+};
+
+__device__ __forceinline__ PrimRec load_prim(const DevScene &s, uint32_t id) {
+  const float4 *p = s.prims + 3 * size_t(id);
+  return PrimRec{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+}
+
+// Test a loaded primitive against the ray; closest queries shrink t1 on a
+// hit (the surface's intersect / intersects methods, surface/mesh.cc:730-760,
+// surface/sphere.cc:110-125, surface/tripar.cc:93-115).
+__device__ __forceinline__ bool test_prim(const PrimRec &r, float3 o, float3 d, float t0, float &t1) {
+  const float kind = r.a.w;
   float t, u, v;
-  if (kind == PK_TRI) {
-    const float4 *p = s.tri + 3 * size_t(idx);
-    float4 c = __ldg(p), a = __ldg(p + 1), b = __ldg(p + 2);
-    if (tripar_hit(xyz(c), xyz(a), xyz(b), false, o, d, t0, t1, t, u, v)) {
+  if (kind == float(PRIM_SPHERE)) {
+    if (sphere_hit(xyz(r.a), r.b.x, o, d, t0, t1, t)) {
       t1 = t;
       return true;
     }
-  } else if (kind == PK_SPHERE) {
-    float4 sp = __ldg(s.sph + idx);
-    if (sphere_hit(xyz(sp), sp.w, o, d, t0, t1, t)) {
-      t1 = t;
-      return true;
-    }
-  } else {
-    const float4 *p = s.tpar + 3 * size_t(idx);
-    float4 c = __ldg(p), a = __ldg(p + 1), b = __ldg(p + 2);
-    if (tripar_hit(xyz(c), xyz(a), xyz(b), c.w != 0.f, o, d, t0, t1, t, u, v)) {
-      t1 = t;
-      return true;
-    }
+    return false;
+  }
+  if (tripar_hit(xyz(r.a), xyz(r.b), xyz(r.c), kind == float(PRIM_PARALLELOGRAM), o, d, t0, t1, t, u, v)) {
+    t1 = t;
+    return true;
   }
   return false;
 }
@@ -193,21 +193,36 @@ __device__ __forceinline__ bool gate_open(uint32_t cb, float t0, float t1, float
   return gx && gy && gz;
 }
 
-// Traverse the octree.  ANY = stop at the first hit (Space::intersects /
-// occludes).  Returns the surviving hit's packed reference, or PREF_END.
-// t1 is shrunk to the closest hit for closest queries.  STACK entries must
-// cover 3 * depth + 2 (chosen by the host from the tree depth); if they do
-// not, cnt.overflow is set and the result must be discarded.
-template <bool ANY, int STACK>
-__device__ uint32_t traverse(const DevScene &s, float3 o, float3 d, float t0, float &t1,
-                             TraceCounters &cnt) {
-  if (s.n_nodes == 0) return PREF_END;
+// A resumable octree walk for one ray.  init() sets up the root's slab
+// bounds (space/octree.cc:119-135); each step() processes one octree entry --
+// the child entered last, else the top of the stack -- exactly as one call of
+// the reference's recursive function does: parent gate, slab cull, the
+// node's surface list, then the children.  Kernels interleave the steps of
+// many rays per warp and refill lanes whose ray has finished.
+// ANY = stop at the first hit (Space::intersects / occludes).  STACK entries
+// must cover 3 * depth + 2 (chosen by the host from the tree depth); if they
+// do not, cnt.overflow is set and the result must be discarded.
+template <int STACK>
+struct Traversal {
+  float3 o, d, lo, hi;
+  float t0, t1;
+  uint32_t node, gate, octant, hit_ref;
+  uint32_t lp, lend;         // surface list still to test: plist[lp, lend)
+  int sp;
+  bool have;                 // a current entry (node/gate/lo/hi) is set
   StackEntry stk[STACK];
-  int sp = 0;
 
-  // Root slab bounds (space/octree.cc:119-135).
-  float3 lo, hi;
-  {
+  __device__ __forceinline__ void init(const DevScene &s, float3 o_, float3 d_, float t0_, float t1_) {
+    o = o_;
+    d = d_;
+    t0 = t0_;
+    t1 = t1_;
+    hit_ref = PREF_END;
+    sp = 0;
+    node = 0;
+    gate = 0;
+    lp = lend = 0;
+    have = s.n_nodes != 0;
     float inv = (d.x == 0.f) ? 1e9f : __fdiv_rn(1.0f, d.x);
     float a = __fmul_rn(__fsub_rn(s.origin[0], o.x), inv);
     float b = __fmul_rn(__fadd_rn(__fsub_rn(s.origin[0], o.x), s.size), inv);
@@ -223,12 +238,61 @@ __device__ uint32_t traverse(const DevScene &s, float3 o, float3 d, float t0, fl
     b = __fmul_rn(__fadd_rn(__fsub_rn(s.origin[2], o.z), s.size), inv);
     if (a > b) { float tmp = a; a = b; b = tmp; }
     lo.z = a; hi.z = b;
+    octant = (d.x >= 0.f ? 0u : 4u) | (d.y >= 0.f ? 0u : 2u) | (d.z >= 0.f ? 0u : 1u);
   }
-  const uint32_t octant = (d.x >= 0.f ? 0u : 4u) | (d.y >= 0.f ? 0u : 2u) | (d.z >= 0.f ? 0u : 1u);
-  uint32_t node = 0, gate = 0;
-  uint32_t hit_ref = PREF_END;
 
-  for (;;) {
+  // One unit of work: the next surface of the pending list if any, else one
+  // octree entry (the child entered last, else the top of the stack).
+  // Returns true when the walk is over (hit_ref / t1 final).
+  //
+  // An entry is processed as one call of the reference's recursive function:
+  // parent gate, slab cull, then the node's surface list, then its children.
+  // Here the qualifying children are pushed when the node is visited and its
+  // list is tested in the following steps; the push uses the ray's extent
+  // before those tests, which only admits more children (the ray can only
+  // shrink), and every entry's gate and cull are evaluated again when it is
+  // entered -- so the tests and their order are the reference's.
+  template <bool ANY>
+  __device__ __forceinline__ bool step(const DevScene &s, TraceCounters &cnt) {
+    if (lp < lend) {
+      // Up to four surfaces of the list per step: one 128-bit load of ids
+      // (lists are 4-aligned), all records fetched before the first test,
+      // then tested in list order.
+      const uint4 ids = __ldg(reinterpret_cast<const uint4 *>(s.plist + lp));
+      const uint32_t nv = lend - lp < 4u ? lend - lp : 4u;
+      PrimRec r0 = load_prim(s, ids.x), r1, r2, r3;
+      if (nv > 1) r1 = load_prim(s, ids.y);
+      if (nv > 2) r2 = load_prim(s, ids.z);
+      if (nv > 3) r3 = load_prim(s, ids.w);
+      lp += 4;
+      cnt.tests += nv;
+      if (test_prim(r0, o, d, t0, t1)) {
+        hit_ref = ids.x;
+        if (ANY) return true;
+      }
+      if (nv > 1 && test_prim(r1, o, d, t0, t1)) {
+        hit_ref = ids.y;
+        if (ANY) return true;
+      }
+      if (nv > 2 && test_prim(r2, o, d, t0, t1)) {
+        hit_ref = ids.z;
+        if (ANY) return true;
+      }
+      if (nv > 3 && test_prim(r3, o, d, t0, t1)) {
+        hit_ref = ids.w;
+        if (ANY) return true;
+      }
+      return lp >= lend && !have && sp == 0;
+    }
+    if (!have) {
+      if (sp == 0) return true;
+      --sp;
+      node = __float_as_uint(stk[sp].lo.w);
+      gate = __float_as_uint(stk[sp].hi.w);
+      lo = xyz(stk[sp].lo);
+      hi = xyz(stk[sp].hi);
+    }
+    have = false;
     bool open = true;
     if (gate & kGateFlag) open = gate_open(gate & 7u, t0, t1, lo, hi);
     if (open) {
@@ -236,37 +300,33 @@ __device__ uint32_t traverse(const DevScene &s, float3 o, float3 d, float t0, fl
       open = slab_open(t0, t1, lo, hi);
     }
     if (open) {
-      uint32_t h = __ldg(s.node_heads + node);
-      if (h) {
-        for (uint32_t ref = __ldg(s.plist + h); ref != PREF_END; ref = __ldg(s.plist + (++h))) {
-          cnt.tests++;
-          if (test_ref(s, ref, o, d, t0, t1)) {
-            hit_ref = ref;
-            if (ANY) return hit_ref;
-          }
-        }
-      }
-      const uint4 *kp = reinterpret_cast<const uint4 *>(s.node_children + 8 * size_t(node));
-      uint4 k0 = __ldg(kp), k1 = __ldg(kp + 1);
-      const bool leaf = (k0.x == 1u && k0.y == 1u);
-      if (!leaf) {
-        float3 half = f3(__fdiv_rn(__fsub_rn(hi.x, lo.x), 2.0f), __fdiv_rn(__fsub_rn(hi.y, lo.y), 2.0f),
-                         __fdiv_rn(__fsub_rn(hi.z, lo.z), 2.0f));
+      const uint4 nd = __ldg(s.nodes + node);
+      lp = nd.z;
+      lend = nd.z + nd.w;
+      if (nd.y) {
+        const float3 half = f3(__fdiv_rn(__fsub_rn(hi.x, lo.x), 2.0f), __fdiv_rn(__fsub_rn(hi.y, lo.y), 2.0f),
+                               __fdiv_rn(__fsub_rn(hi.z, lo.z), 2.0f));
+        // Per axis the children's bounds take two values each: the near
+        // half spans [lo, lo + half], the far half [lo + half, lo + half +
+        // half] -- the same rounded sums as the reference's child ranges.
+        const float3 mid = f3(__fadd_rn(lo.x, half.x), __fadd_rn(lo.y, half.y), __fadd_rn(lo.z, half.z));
+        const float3 far = f3(__fadd_rn(mid.x, half.x), __fadd_rn(mid.y, half.y), __fadd_rn(mid.z, half.z));
+        const float3 near_lo = f3(__fadd_rn(lo.x, 0.f), __fadd_rn(lo.y, 0.f), __fadd_rn(lo.z, 0.f));
         // Walk the visiting order backwards: every qualifying child but the
         // first is pushed (so they pop in visiting order after the first
-        // child's subtree), the first is entered directly.  At most 4 pass
-        // (one octant per crossing of each of the three midplanes).
-        bool have = false;
+        // child's subtree), the first becomes the current entry.  At most 4
+        // pass (one octant per crossing of each of the three midplanes).
         StackEntry pend;
 #pragma unroll
         for (int i = 7; i >= 0; i--) {
           const uint32_t cb = (i == 3) ? 4u : (i == 4) ? 3u : uint32_t(i);
-          const uint32_t c = pick_child(k0, k1, cb ^ octant);
-          if (!c) continue;
-          float3 clo = f3(__fadd_rn(lo.x, (cb & 4) ? half.x : 0.f), __fadd_rn(lo.y, (cb & 2) ? half.y : 0.f),
-                          __fadd_rn(lo.z, (cb & 1) ? half.z : 0.f));
-          float3 chi = f3(__fadd_rn(clo.x, half.x), __fadd_rn(clo.y, half.y), __fadd_rn(clo.z, half.z));
+          const uint32_t slot = cb ^ octant;
+          if (!((nd.y >> slot) & 1u)) continue;
+          const float3 clo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y,
+                                (cb & 1) ? mid.z : near_lo.z);
+          const float3 chi = f3((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z);
           if (!gate_open(cb, t0, t1, clo, chi) || !slab_open(t0, t1, clo, chi)) continue;
+          const uint32_t c = nd.x + __popc(nd.y & ((1u << slot) - 1u));
           if (have) {
             if (sp < STACK) stk[sp++] = pend;
             else cnt.overflow = 1;
@@ -280,28 +340,57 @@ __device__ uint32_t traverse(const DevScene &s, float3 o, float3 d, float t0, fl
           gate = __float_as_uint(pend.hi.w);
           lo = xyz(pend.lo);
           hi = xyz(pend.hi);
-          continue;
         }
       }
     }
-    if (sp == 0) break;
-    --sp;
-    node = __float_as_uint(stk[sp].lo.w);
-    gate = __float_as_uint(stk[sp].hi.w);
-    lo = xyz(stk[sp].lo);
-    hi = xyz(stk[sp].hi);
+    return lp >= lend && !have && sp == 0;
   }
-  return hit_ref;
-}
+};
+
+// Warp-cooperative ray dispenser for the persistent trace kernels: lanes
+// whose ray is finished take the next index from a warp-local range of CHUNK
+// rays, refilled with one atomic on the launch's counter.  All 32 lanes of
+// the warp must call fetch() together.
+struct RayDispenser {
+  static constexpr uint32_t kChunk = 64;
+  static constexpr uint32_t kIdle = 0xffffffffu;
+  uint32_t next = 0, end = 0;
+  bool exhausted = false;
+
+  // Returns the new ray index for a lane that asked (NEED) and got one,
+  // else kIdle.  Sets *all_idle when every lane is idle and no rays remain.
+  __device__ __forceinline__ uint32_t fetch(uint32_t *counter, uint32_t n, bool need, bool busy,
+                                            bool *all_idle) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t mask = __ballot_sync(0xffffffffu, need);
+    uint32_t got = kIdle;
+    if (mask) {
+      if (next >= end && !exhausted) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(counter, kChunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) {
+          exhausted = true;
+        } else {
+          next = base;
+          end = base + kChunk < n ? base + kChunk : n;
+        }
+      }
+      const uint32_t rank = __popc(mask & ((1u << lane) - 1u));
+      if (need && next + rank < end) got = next + rank;
+      const uint32_t take = __popc(mask);
+      next = (next + take < end) ? next + take : end;
+    }
+    const bool idle = !busy && got == kIdle;
+    *all_idle = __all_sync(0xffffffffu, idle) && exhausted && next >= end;
+    return got;
+  }
+};
 
 // Global primitive id of a packed reference: triangles, then spheres, then
 // tripars.
-__device__ __forceinline__ int32_t prim_id_of(const DevScene &s, uint32_t ref) {
-  if (ref == PREF_END) return -1;
-  uint32_t kind = ref >> 30, idx = ref & PREF_INDEX_MASK;
-  if (kind == PK_TRI) return int32_t(idx);
-  if (kind == PK_SPHERE) return int32_t(s.n_tri + idx);
-  return int32_t(s.n_tri + s.n_sph + idx);
+__device__ __forceinline__ int32_t prim_id_of(const DevScene &, uint32_t ref) {
+  return ref == PREF_END ? -1 : int32_t(ref);
 }
 
 }  // namespace snog

@@ -107,6 +107,7 @@ __global__ void __launch_bounds__(256) k_camera(JobConsts jc, uint64_t base, uin
     counters[0] = n;
     counters[1] = 0;
     counters[2] = 0;
+    counters[4] = 0;          // closest kernel's dispenser
   }
   const Strata st = strata_for(jc.S);
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -147,56 +148,79 @@ __device__ __forceinline__ void warp_count(unsigned long long *p, unsigned long 
   }
 }
 
+// Persistent closest-hit kernel: warps take rays from the queue through a
+// RayDispenser (counters[4]) and interleave one octree entry per ray per
+// iteration, so finished lanes are refilled instead of idling.
 template <int STACK>
-__global__ void __launch_bounds__(128) k_trace_closest(DevScene s, RayQ q, uint32_t *counters, uint32_t cur,
+__global__ void __launch_bounds__(128, 6) k_trace_closest(DevScene s, RayQ q, uint32_t *counters, uint32_t cur,
                                                        uint32_t *hit_ref, float *hit_t,
                                                        unsigned long long *stats, bool prof) {
   const uint32_t n = counters[cur];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     counters[cur ^ 1u] = 0;   // next queue and shadow queue start empty
     counters[2] = 0;
+    counters[5] = 0;          // shadow kernel's dispenser
     stats[0] += n;
   }
   unsigned long long nodes = 0, tests = 0;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    float4 o = q.o[i], d = q.d[i];
-    float t1 = d.w;
-    TraceCounters c{0, 0, 0};
-    uint32_t ref = traverse<false, STACK>(s, xyz(o), xyz(d), o.w, t1, c);
-    hit_ref[i] = ref;
-    hit_t[i] = t1;
-    if (c.overflow) atomicOr(counters + 3, 1u);
-    nodes += c.nodes;
-    tests += c.tests;
+  Traversal<STACK> tr;
+  RayDispenser disp;
+  uint32_t ray = RayDispenser::kIdle;
+  TraceCounters c{0, 0, 0};
+  for (;;) {
+    bool all_idle;
+    const uint32_t got = disp.fetch(counters + 4, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle,
+                                    &all_idle);
+    if (all_idle) break;
+    if (got != RayDispenser::kIdle) {
+      ray = got;
+      const float4 o = q.o[ray], d = q.d[ray];
+      tr.init(s, xyz(o), xyz(d), o.w, d.w);
+    }
+    if (ray == RayDispenser::kIdle) continue;
+    if (!tr.template step<false>(s, c)) continue;
+    hit_ref[ray] = tr.hit_ref;
+    hit_t[ray] = tr.t1;
+    ray = RayDispenser::kIdle;
   }
-  if (prof) warp_count(stats + 2, nodes, tests);
+  if (c.overflow) atomicOr(counters + 3, 1u);
+  if (prof) warp_count(stats + 2, c.nodes, c.tests);
 }
 
+// Persistent any-hit kernel for the shadow queue (dispenser counters[5]);
+// an unoccluded ray adds its contribution to its path's radiance.
 template <int STACK>
-__global__ void __launch_bounds__(128) k_trace_shadow(DevScene s, ShadowQ q, uint32_t *counters, float4 *rad,
+__global__ void __launch_bounds__(128, 6) k_trace_shadow(DevScene s, ShadowQ q, uint32_t *counters, float4 *rad,
                                                       unsigned long long *stats, bool prof) {
   const uint32_t n = counters[2];
   if (blockIdx.x == 0 && threadIdx.x == 0) stats[1] += n;
-  unsigned long long nodes = 0, tests = 0;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    float4 o = q.o[i], d = q.d[i];
-    float t1 = d.w;
-    TraceCounters c{0, 0, 0};
-    uint32_t ref = traverse<true, STACK>(s, xyz(o), xyz(d), o.w, t1, c);
-    if (c.overflow) atomicOr(counters + 3, 1u);
-    nodes += c.nodes;
-    tests += c.tests;
-    if (ref == PREF_END) {
-      float4 cc = q.c[i];
+  Traversal<STACK> tr;
+  RayDispenser disp;
+  uint32_t ray = RayDispenser::kIdle;
+  TraceCounters c{0, 0, 0};
+  for (;;) {
+    bool all_idle;
+    const uint32_t got = disp.fetch(counters + 5, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle,
+                                    &all_idle);
+    if (all_idle) break;
+    if (got != RayDispenser::kIdle) {
+      ray = got;
+      const float4 o = q.o[ray], d = q.d[ray];
+      tr.init(s, xyz(o), xyz(d), o.w, d.w);
+    }
+    if (ray == RayDispenser::kIdle) continue;
+    if (!tr.template step<true>(s, c)) continue;
+    if (tr.hit_ref == PREF_END) {
+      float4 cc = q.c[ray];
       float4 *r = rad + __float_as_uint(cc.w);
       atomicAdd(&r->x, cc.x);
       atomicAdd(&r->y, cc.y);
       atomicAdd(&r->z, cc.z);
     }
+    ray = RayDispenser::kIdle;
   }
-  if (prof) warp_count(stats + 4, nodes, tests);
+  if (c.overflow) atomicOr(counters + 3, 1u);
+  if (prof) warp_count(stats + 4, c.nodes, c.tests);
 }
 
 __device__ __forceinline__ float3 medium_transmittance(const DevMedium &m, float len) {
@@ -210,6 +234,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene s, JobConsts jc, uint64_
                                                const uint32_t *hit_ref, const float *hit_t, PathPtrs P,
                                                RayQ qout, ShadowQ sq) {
   const uint32_t n = counters[cur];
+  if (blockIdx.x == 0 && threadIdx.x == 0) counters[4] = 0;   // next bounce's dispenser
   uint32_t *count_out = counters + (cur ^ 1u);
   uint32_t *count_sq = counters + 2;
   const uint32_t lane = threadIdx.x & 31u;
@@ -500,11 +525,11 @@ void launch_bounce(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, uint
   PathPtrs P{wb.thr, wb.rad, wb.pstate, wb.jit};
   const bool pf = prof != nullptr;
   if (pf) prof->begin(st, RenderProfile::CLOSEST);
-  k_trace_closest<STACK><<<grid128, 128, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
+  k_trace_closest<STACK><<<resident_grid(k_trace_closest<STACK>, 128), 128, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
   if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADE);
   k_shade<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, P, qout, sq);
   if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADOW);
-  k_trace_shadow<STACK><<<grid128, 128, 0, st>>>(s, sq, wb.counters, wb.rad, wb.stats, pf);
+  k_trace_shadow<STACK><<<resident_grid(k_trace_shadow<STACK>, 128), 128, 0, st>>>(s, sq, wb.counters, wb.rad, wb.stats, pf);
   if (pf) prof->end(st);
 }
 

@@ -207,6 +207,19 @@ int snog_render_device(SnogScene *scene, const SnogCamera *camera,
                        const SnogRenderParams *params, float *d_out_rgb, void *stream,
                        SnogRenderStats *stats);
 
+/* The same render as snog_render_device, but the library allocates no device
+ * memory: all working memory comes from one fixed 64 MiB device array that
+ * the library holds (per GPU) until the process exits.  No counterpart in the
+ * reference, which renders on the CPU.  For hosts that manage every byte of
+ * device memory themselves, or cannot let cudaMalloc/cudaFree stall the
+ * device mid-loop.  Limits: at most 1048576 output pixels, and a wave of the
+ * scratch must hold one pixel's samples; larger jobs return SNOG_EINVAL.  The
+ * first call on a device looks up the array's address and should come before
+ * any stream capture.  Calls share the array: calls whose work overlaps on
+ * the GPU race and must be ordered by the caller (e.g. one stream). */
+int snog_render_device_noalloc(SnogScene *scene, const SnogCamera *camera,
+                               const SnogRenderParams *params, float *d_out_rgb, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

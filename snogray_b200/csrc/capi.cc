@@ -15,10 +15,6 @@
 #include "launch.h"
 #include "scene.h"
 
-struct SnogScene {
-  snog::SceneImpl *impl;
-};
-
 namespace snog {
 
 thread_local std::string g_last_error;

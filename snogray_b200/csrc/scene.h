@@ -62,4 +62,9 @@ void check_cuda(int err, const char *what);   // throws Error{SNOG_ECUDA}
 
 }  // namespace snog
 
+// The opaque handle of the C ABI.
+struct SnogScene {
+  snog::SceneImpl *impl;
+};
+
 #endif

@@ -47,7 +47,7 @@ def build(targets=("all",), quiet=True):
 
 
 def ensure_port():
-    if not os.access(port_binary(), os.X_OK) or not os.path.exists(os.path.join(REF_DIR, "libsnogport.so")):
+    if not os.access(port_binary(), os.X_OK):
         build(["port"])
     return port_binary()
 

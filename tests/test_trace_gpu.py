@@ -115,6 +115,25 @@ def test_trace_empty_batch():
     assert prim.size == 0 and cnt["closest_nodes"] == 0
 
 
+def test_trace_full_size_batch_matches_restatement():
+    """The intersection-only workload at full size -- 1M random triangles,
+    16M rays (origins U[-0.1,1.1]^3, directions uniform, t_max = inf), half
+    closest-hit, half any-hit -- every id and every closest-hit distance
+    equal to the oracle's restatement run on this machine's CPU cores."""
+    import os
+    sd = scenes.random_triangles(1 << 20, seed=2)
+    rays = scenes.random_rays(1 << 24, seed=3)
+    nc = rays.shape[1] // 2
+    ref_prim, ref_t, _, _, _ = spec.port_trace(sd, rays, nc, threads=os.cpu_count() or 8)
+    with Scene(sd) as sc:
+        prim, t, _, _ = sc.trace(rays, nc)
+    bad = np.nonzero(prim != ref_prim)[0]
+    assert len(bad) == 0, f"{len(bad)} id mismatches of {len(prim)}"
+    hit = np.nonzero(prim[:nc] >= 0)[0]
+    assert np.array_equal(t[hit].view(np.uint32), ref_t[hit].view(np.uint32))
+    assert 0.5 < len(hit) / nc < 0.9
+
+
 @pytest.mark.skipif(not spec.have_ref(), reason="compiled reference not present")
 def test_trace_large_soup_matches_live_reference():
     """200k triangles, 262k rays: ids bit-exact against the reference run

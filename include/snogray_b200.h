@@ -207,6 +207,68 @@ int snog_render_device(SnogScene *scene, const SnogCamera *camera,
                        const SnogRenderParams *params, float *d_out_rgb, void *stream,
                        SnogRenderStats *stats);
 
+/* ---- Batched and served rendering ---------------------------------------
+ * The streaming engine traces many jobs (scene, camera, size, samples) in one
+ * persistent wavefront with path regeneration: paths of all admitted jobs
+ * share the ray queues, finished paths are replaced at once by new camera
+ * paths from a device work ring of (job, path range) items, and each
+ * iteration's kernel sequence is a CUDA graph.  It replaces RenderMgr's
+ * packet queue and render threads (render-mgr/render-mgr.cc:126-256) for many
+ * renders at once; each job's image equals its plain render (snog_render) up
+ * to float summation order. */
+typedef struct SnogEngineConfig {
+  uint32_t slots;             /* paths in flight (ray queue capacity) */
+  uint32_t item_paths;        /* paths per work item (the scheduling grain) */
+  uint32_t ring_items;        /* work ring capacity, items */
+  uint32_t max_jobs;          /* jobs admitted at once */
+  uint32_t max_lights;        /* light samples per vertex (lights x direct_samples) */
+  uint32_t iters_per_launch;  /* iteration pairs per graph launch */
+  uint64_t mem_budget;        /* device bytes for per-job buffers (admission) */
+} SnogEngineConfig;
+
+typedef struct SnogJobStats {
+  double submit_ms, admit_ms, start_ms, finish_ms;   /* engine clock */
+  uint64_t paths;                                    /* width x height x spp */
+  int32_t status;                                    /* SNOG_OK, SNOG_EBUSY, SNOG_ECANCELED */
+} SnogJobStats;
+
+typedef struct SnogBatchStats {
+  uint64_t paths, closest_rays, shadow_rays;
+  double wall_ms;
+  uint32_t kernel_launches;
+} SnogBatchStats;
+
+/* Defaults: 16M slots, 64K-path items, 16K-item ring, 4096 jobs, 4 light
+ * samples, 4 iteration pairs per launch, 120 GB budget. */
+int snog_engine_default_config(SnogEngineConfig *cfg);
+
+/* Render N_JOBS jobs together to completion.  outs[i] receives job i's image
+ * (height x width RGB floats, top row first) in host memory, or device memory
+ * if outs_on_device.  cfg may be NULL for defaults. */
+int snog_render_batch(SnogScene *const *scenes, const SnogCamera *cameras, const SnogRenderParams *params,
+                      uint32_t n_jobs, float *const *outs, int outs_on_device, const SnogEngineConfig *cfg,
+                      SnogBatchStats *stats);
+
+/* A render server: a background thread drives the engine; jobs submitted
+ * while others run are admitted as job slots and the memory budget allow and
+ * interleave with them (continuous batching).  No counterpart in the
+ * reference (which renders one image per process). */
+typedef struct SnogServer SnogServer;
+int snog_server_create(const SnogEngineConfig *cfg, SnogServer **out);
+/* Make SCENE resident in the server; jobs name it by the returned slot. */
+int snog_server_add_scene(SnogServer *server, SnogScene *scene, uint32_t *slot);
+/* Queue a job; its image goes to HOST_OUT (height x width RGB floats) when done. */
+int snog_server_submit(SnogServer *server, uint32_t slot, const SnogCamera *camera,
+                       const SnogRenderParams *params, float *host_out, uint64_t *job_id);
+/* SNOG_OK when the job is finished (stats filled), SNOG_EBUSY while it is not,
+ * SNOG_ECANCELED / SNOG_ENOTFOUND. */
+int snog_server_poll(SnogServer *server, uint64_t job_id, SnogJobStats *stats);
+/* Wait up to timeout_ms; SNOG_ETIMEOUT if the job is still running. */
+int snog_server_wait(SnogServer *server, uint64_t job_id, uint32_t timeout_ms, SnogJobStats *stats);
+int snog_server_cancel(SnogServer *server, uint64_t job_id);
+/* Stops the server thread (finishing nothing further) and frees it. */
+int snog_server_destroy(SnogServer *server);
+
 /* The same render as snog_render_device, but the library allocates no device
  * memory: all working memory comes from one fixed 64 MiB device array that
  * the library holds (per GPU) until the process exits.  No counterpart in the

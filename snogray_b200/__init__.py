@@ -88,6 +88,22 @@ class SnogRenderStats(C.Structure):
                 ("shadow_tests", C.c_uint64)]
 
 
+class SnogEngineConfig(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("item_paths", C.c_uint32), ("ring_items", C.c_uint32),
+                ("max_jobs", C.c_uint32), ("max_lights", C.c_uint32), ("iters_per_launch", C.c_uint32),
+                ("mem_budget", C.c_uint64)]
+
+
+class SnogJobStats(C.Structure):
+    _fields_ = [("submit_ms", C.c_double), ("admit_ms", C.c_double), ("start_ms", C.c_double),
+                ("finish_ms", C.c_double), ("paths", C.c_uint64), ("status", C.c_int32)]
+
+
+class SnogBatchStats(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("wall_ms", C.c_double), ("kernel_launches", C.c_uint32)]
+
+
 def _sig(name, res, *args):
     try:
         f = getattr(_lib, name)
@@ -115,6 +131,20 @@ _render = _sig("snog_render", C.c_int, _P, C.POINTER(SnogCamera), C.POINTER(Snog
                C.POINTER(SnogRenderStats))
 _render_device = _sig("snog_render_device", C.c_int, _P, C.POINTER(SnogCamera),
                       C.POINTER(SnogRenderParams), _P, _P, C.POINTER(SnogRenderStats))
+
+
+_engine_default = _sig("snog_engine_default_config", C.c_int, C.POINTER(SnogEngineConfig))
+_render_batch = _sig("snog_render_batch", C.c_int, C.POINTER(_P), C.POINTER(SnogCamera),
+                     C.POINTER(SnogRenderParams), C.c_uint32, C.POINTER(_P), C.c_int,
+                     C.POINTER(SnogEngineConfig), C.POINTER(SnogBatchStats))
+_server_create = _sig("snog_server_create", C.c_int, C.POINTER(SnogEngineConfig), C.POINTER(_P))
+_server_add_scene = _sig("snog_server_add_scene", C.c_int, _P, _P, C.POINTER(C.c_uint32))
+_server_submit = _sig("snog_server_submit", C.c_int, _P, C.c_uint32, C.POINTER(SnogCamera),
+                      C.POINTER(SnogRenderParams), _P, C.POINTER(C.c_uint64))
+_server_poll = _sig("snog_server_poll", C.c_int, _P, C.c_uint64, C.POINTER(SnogJobStats))
+_server_wait = _sig("snog_server_wait", C.c_int, _P, C.c_uint64, C.c_uint32, C.POINTER(SnogJobStats))
+_server_cancel = _sig("snog_server_cancel", C.c_int, _P, C.c_uint64)
+_server_destroy = _sig("snog_server_destroy", C.c_int, _P)
 
 
 def _check(rc):
@@ -258,6 +288,93 @@ class Scene:
         _check(_render_device(self._h, C.byref(cs), C.byref(ps), d_out, stream,
                               C.byref(st) if want_stats else None))
         return {f: getattr(st, f) for f, _ in SnogRenderStats._fields_} if want_stats else None
+
+
+def engine_config(**kw):
+    """The engine's default configuration with fields overridden by KW."""
+    c = SnogEngineConfig()
+    _check(_engine_default(C.byref(c)))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def render_batch(jobs, config=None):
+    """Render [(Scene, Camera, RenderParams), ...] together on the streaming
+    engine.  Returns (list of (H, W, 3) float32 images, stats dict)."""
+    n = len(jobs)
+    scenes = (_P * n)(*[j[0].handle for j in jobs])
+    cams = (SnogCamera * n)(*[camera_struct(j[1]) for j in jobs])
+    prms = (SnogRenderParams * n)(*[params_struct(j[2]) for j in jobs])
+    outs = [np.empty((j[2].height, j[2].width, 3), np.float32) for j in jobs]
+    optr = (_P * n)(*[o.ctypes.data for o in outs])
+    st = SnogBatchStats()
+    _check(_render_batch(scenes, cams, prms, n, optr, 0, C.byref(config) if config else None,
+                         C.byref(st)))
+    return outs, {f: getattr(st, f) for f, _ in SnogBatchStats._fields_}
+
+
+class Server:
+    """A render server (snog_server_*): scenes stay resident, jobs submitted
+    at any time join the running wavefront (continuous batching)."""
+
+    def __init__(self, config=None):
+        h = _P()
+        _check(_server_create(C.byref(config) if config else None, C.byref(h)))
+        self._h = h
+        self._outs = {}
+        self._scenes = []
+
+    def add_scene(self, scene: Scene):
+        slot = C.c_uint32()
+        _check(_server_add_scene(self._h, scene.handle, C.byref(slot)))
+        self._scenes.append(scene)
+        return slot.value
+
+    def submit(self, slot, camera: Camera, params: RenderParams):
+        out = np.empty((params.height, params.width, 3), np.float32)
+        jid = C.c_uint64()
+        cs, ps = camera_struct(camera), params_struct(params)
+        _check(_server_submit(self._h, slot, C.byref(cs), C.byref(ps), out.ctypes.data, C.byref(jid)))
+        self._outs[jid.value] = out
+        return jid.value
+
+    @staticmethod
+    def _stats(st):
+        return {f: getattr(st, f) for f, _ in SnogJobStats._fields_}
+
+    def poll(self, job):
+        st = SnogJobStats()
+        rc = _server_poll(self._h, job, C.byref(st))
+        if rc == SNOG_EBUSY:
+            return None
+        _check(rc)
+        return self._outs.pop(job), self._stats(st)
+
+    def wait(self, job, timeout_ms=60000):
+        st = SnogJobStats()
+        _check(_server_wait(self._h, job, timeout_ms, C.byref(st)))
+        return self._outs.pop(job), self._stats(st)
+
+    def cancel(self, job):
+        _check(_server_cancel(self._h, job))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(_server_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def exported_symbols():

@@ -1,0 +1,716 @@
+// engine.cu -- kernels and host loop of the streaming render engine
+// (engine.h).  The per-vertex shading is the same as the wave renderer's
+// (wavefront.cu) -- PathInteg::Li, render/path-integ.cc:134-407 -- with the
+// path's job, scene and bounce carried in its queue entry, so one launch
+// serves many jobs at different depths.  Random streams are keyed by (job
+// seed, path index in the job, dimension) exactly as in the wave renderer, so
+// a job renders the same image (up to float summation order) either way.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "engine.h"
+#include "launch.h"
+#include "pathstate.cuh"
+
+namespace snog {
+
+namespace {
+
+struct EQ {                 // one ray queue, SoA of 16-byte records
+  float4 *o, *d, *thr, *rad;
+  uint4 *meta;              // x = path state, y = job, z/w = path index lo/hi
+};
+
+struct ESQ {                // shadow queue
+  float4 *o, *d, *c;        // c.w = scene index
+  unsigned long long *tgt;  // address of the float4 radiance to add to
+};
+
+__global__ void k_e_plan(EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N, uint32_t cur) {
+  const uint32_t n_cur = ctl->qcount[cur];
+  const unsigned long long avail = ctl->avail_end - ctl->ticket;
+  unsigned long long n_new = N - n_cur;
+  if (n_new > avail) n_new = avail;
+  // Retire items fully consumed before this iteration's tickets.
+  unsigned long long head = ctl->item_head;
+  while (head < ctl->item_tail) {
+    const WorkItem &w = ring[head % R];
+    if (w.cum + w.count > ctl->ticket) break;
+    head++;
+  }
+  ctl->item_head = head;
+  ctl->regen_start = ctl->ticket;
+  ctl->regen_n = uint32_t(n_new);
+  ctl->regen_base = n_cur;
+  ctl->ticket += n_new;
+  ctl->paths_started += n_new;
+  ctl->qcount[cur] = n_cur + uint32_t(n_new);
+  ctl->qcount[cur ^ 1u] = 0;
+  ctl->scount = 0;
+  ctl->disp_closest = 0;
+  ctl->disp_shadow = 0;
+}
+
+// New camera paths for tickets [regen_start, regen_start + regen_n).
+__global__ void __launch_bounds__(256) k_e_regen(EngineCtl *ctl, const WorkItem *ring, uint32_t R,
+                                                 const EngineJobDev *jobs, EQ q) {
+  const uint32_t n = ctl->regen_n;
+  const unsigned long long t0 = ctl->regen_start, head = ctl->item_head, tail = ctl->item_tail;
+  const uint32_t base = ctl->regen_base;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const unsigned long long ticket = t0 + t;
+    // Item holding this ticket: binary search over the ring window.
+    unsigned long long lo = head, hi = tail;   // invariant: answer in [lo, hi)
+    while (hi - lo > 1) {
+      const unsigned long long mid = lo + (hi - lo) / 2;
+      if (ring[mid % R].cum <= ticket) lo = mid;
+      else hi = mid;
+    }
+    const WorkItem w = ring[lo % R];
+    const uint32_t job = w.job;
+    const unsigned long long g = w.begin + (ticket - w.cum);
+    const EngineJobDev &J = jobs[job];
+    const JobConsts &jc = J.jc;
+    const uint32_t pixel = uint32_t(g / jc.S), s = uint32_t(g % jc.S);
+    const int px = int(pixel % jc.PW) - 2, py = int(pixel / jc.PW) - 2;
+    Rng rng{jc.seed_lo, jc.seed_hi, uint32_t(g), uint32_t(g >> 32)};
+    const float2 j = strat_uv(strata_for(jc.S), rng, pixel, s, dim_of(0, K_CAMERA));
+    // Renderer::render_packet (render-mgr/renderer.cc:69-88), Camera::eye_vec (camera/camera.h:384-389)
+    const float cu = float(px) + j.x, cv = float(py) + j.y;
+    const float fu = cu / float(jc.W), fv = (float(jc.H) - cv) / float(jc.H);
+    const float x = 2.f * fu - 1.f, y = 2.f * fv - 1.f;
+    const float3 d = add(add(load3(jc.cam_fwd), mul(mul(load3(jc.cam_right), x), jc.tan_x)),
+                         mul(mul(load3(jc.cam_up), y), jc.tan_y));
+    const uint32_t slot = base + t;
+    q.o[slot] = make_float4(jc.cam_pos[0], jc.cam_pos[1], jc.cam_pos[2], 0.f);
+    q.d[slot] = make_float4(d.x, d.y, d.z, jc.max_trace);
+    q.thr[slot] = make_float4(1.f, 1.f, 1.f, 1.f);
+    q.rad[slot] = make_float4(0.f, 0.f, 0.f, 1.f);
+    q.meta[slot] = make_uint4(0u, job, uint32_t(g), uint32_t(g >> 32));
+    J.jit[g] = j;
+  }
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128, 6) k_e_closest(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
+                                                      const DevScene *scenes, EQ q, uint32_t *hit_ref,
+                                                      float *hit_t) {
+  const uint32_t n = ctl->qcount[cur];
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_closest += n;
+  Traversal<STACK> tr;
+  RayDispenser disp;
+  uint32_t ray = RayDispenser::kIdle;
+  const DevScene *sc = scenes;
+  TraceCounters c{0, 0, 0};
+  for (;;) {
+    bool all_idle;
+    const uint32_t got =
+        disp.fetch(&ctl->disp_closest, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
+    if (all_idle) break;
+    if (got != RayDispenser::kIdle) {
+      ray = got;
+      sc = scenes + jobs[q.meta[ray].y].scene;
+      const float4 o = q.o[ray], d = q.d[ray];
+      tr.init(*sc, xyz(o), xyz(d), o.w, d.w);
+    }
+    if (ray == RayDispenser::kIdle) continue;
+    if (!tr.template step<false>(*sc, c)) continue;
+    hit_ref[ray] = tr.hit_ref;
+    hit_t[ray] = tr.t1;
+    ray = RayDispenser::kIdle;
+  }
+  if (c.overflow) atomicOr(&ctl->err, 1u);
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128, 6) k_e_shadow(EngineCtl *ctl, const DevScene *scenes, ESQ q) {
+  const uint32_t n = ctl->scount;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_shadow += n;
+  Traversal<STACK> tr;
+  RayDispenser disp;
+  uint32_t ray = RayDispenser::kIdle;
+  const DevScene *sc = scenes;
+  TraceCounters c{0, 0, 0};
+  for (;;) {
+    bool all_idle;
+    const uint32_t got =
+        disp.fetch(&ctl->disp_shadow, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
+    if (all_idle) break;
+    if (got != RayDispenser::kIdle) {
+      ray = got;
+      sc = scenes + __float_as_uint(q.c[ray].w);
+      const float4 o = q.o[ray], d = q.d[ray];
+      tr.init(*sc, xyz(o), xyz(d), o.w, d.w);
+    }
+    if (ray == RayDispenser::kIdle) continue;
+    if (!tr.template step<true>(*sc, c)) continue;
+    if (tr.hit_ref == PREF_END) {
+      const float4 cc = q.c[ray];
+      float *dst = reinterpret_cast<float *>(q.tgt[ray]);
+      atomicAdd(dst, cc.x);
+      atomicAdd(dst + 1, cc.y);
+      atomicAdd(dst + 2, cc.z);
+    }
+    ray = RayDispenser::kIdle;
+  }
+  if (c.overflow) atomicOr(&ctl->err, 1u);
+}
+
+__global__ void __launch_bounds__(128) k_e_shade(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
+                                                 const DevScene *scenes, EQ qin, const uint32_t *hit_ref,
+                                                 const float *hit_t, EQ qout, ESQ sq,
+                                                 unsigned long long *job_done) {
+  const uint32_t n = ctl->qcount[cur];
+  uint32_t *count_out = &ctl->qcount[cur ^ 1u];
+  uint32_t *count_sq = &ctl->scount;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+
+  for (uint32_t wb = warp * 32; wb < n; wb += nwarps * 32) {
+    const uint32_t i = wb + lane;
+    const bool active = i < n;
+    uint32_t ps = 0, ref = PREF_END, job = 0, scene = 0, bounce = 0;
+    unsigned long long g = 0;
+    float4 o4 = make_float4(0, 0, 0, 0), d4 = o4;
+    float3 thr = f3(0, 0, 0), rad = f3(0, 0, 0);
+    float rr_ratio = 1.f, alpha = 1.f;
+    bool alive = false;
+    Isec I;
+    BsdfCtx B{nullptr, 1.f, 1.f};
+    DevMedium med{1.f, {0, 0, 0}};
+    const EngineJobDev *J = jobs;
+    const DevScene *s = scenes;
+    Rng rng{0, 0, 0, 0};
+    uint32_t pixel = 0, sidx = 0;
+    if (active) {
+      const uint4 meta = qin.meta[i];
+      ps = meta.x;
+      job = meta.y;
+      g = (unsigned long long)meta.z | ((unsigned long long)meta.w << 32);
+      J = jobs + job;
+      scene = J->scene;
+      s = scenes + scene;
+      o4 = qin.o[i];
+      d4 = qin.d[i];
+      ref = hit_ref[i];
+      const float t = hit_t[i];
+      const float4 t4 = qin.thr[i], r4 = qin.rad[i];
+      thr = xyz(t4);
+      rr_ratio = t4.w;
+      rad = xyz(r4);
+      alpha = r4.w;
+      const JobConsts &jc = J->jc;
+      rng = Rng{jc.seed_lo, jc.seed_hi, uint32_t(g), uint32_t(g >> 32)};
+      pixel = uint32_t(g / jc.S);
+      sidx = uint32_t(g % jc.S);
+      bounce = ps_len(ps);
+      const uint32_t depth = ps_depth(ps);
+      med = s->media[depth ? ps_medium(ps, depth - 1) : 0u];
+      const float t1 = ref == PREF_END ? d4.w : t;
+      thr = mul3(thr, medium_transmittance(med, length(xyz(d4)) * (t1 - o4.w)));
+      const bool include_emitters = bounce == 0 || ps_spec(ps) || jc.direct_samples == 0;
+      if (ref == PREF_END) {
+        if (include_emitters) rad = add(rad, mul3(background(*s, xyz(d4)), thr));
+        if (bounce == 0 && rad.x == 0.f && rad.y == 0.f && rad.z == 0.f) alpha = jc.bg_alpha;
+      } else {
+        I = make_isec(*s, ref, xyz(o4), xyz(d4), t);
+        const DevMaterial &M = s->mats[I.mat];
+        if (include_emitters && M.type == MAT_GLOW && !I.back) rad = add(rad, mul3(load3(M.color), thr));
+        const DevMaterial *bm = bsdf_material(*s, I.mat);
+        if (bm) {
+          B.m = bm;
+          B.medium_ior = med.ior;
+          B.enclosing_ior = depth >= 2 ? s->media[ps_medium(ps, depth - 2)].ior : 1.f;
+          alive = true;
+        }
+      }
+    }
+
+    // ---- continuation first, so shadow rays know where their path lives --
+    bool cont = false;
+    float3 thr_next = thr, next_d = f3(0, 0, 0);
+    float rr_next = rr_ratio;
+    uint32_t ps_next = ps;
+    if (alive) {
+      const JobConsts &jc = J->jc;
+      const bool strat = bounce < jc.min_len;
+      float2 prm = strat ? strat_uv(strata_for(jc.S), rng, pixel, sidx, dim_of(bounce, K_BSDF))
+                         : rng.uv(dim_of(bounce, K_BSDF));
+      BSample bs = bsdf_sample(B, I, prm, B_ALL);
+      if (bs.pdf != 0.f && !(bs.val.x == 0.f && bs.val.y == 0.f && bs.val.z == 0.f)) {
+        thr_next = mul3(thr, mul(bs.val, fabsf(I.cos_n(bs.dir)) / bs.pdf));
+        bool stop = false;
+        if (bounce > jc.min_len) {
+          float p = fminf(intensity(thr_next) * rr_ratio, 1.f);
+          if (rng.u(dim_of(bounce, K_RR)) > p) {
+            stop = true;
+          } else {
+            thr_next = mul(thr_next, 1.f / p);
+            rr_next = rr_ratio * p;
+          }
+        }
+        if (!stop && bounce != jc.max_len) {
+          cont = true;
+          next_d = I.nf.from(bs.dir);
+          uint32_t nps = (ps & ~0x1ffu) | (bounce + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
+          if (bs.flags & B_TRANSMISSIVE) {
+            const uint32_t mid = s->mats[I.mat].medium_id;
+            if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
+          }
+          ps_next = nps;
+        }
+      }
+    }
+    const uint32_t slot = warp_append(count_out, cont);
+    float4 *target = nullptr;
+    if (active) {
+      if (cont) {
+        const JobConsts &jc = J->jc;
+        qout.o[slot] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+        qout.d[slot] = make_float4(next_d.x, next_d.y, next_d.z, jc.horizon);
+        qout.thr[slot] = make_float4(thr_next.x, thr_next.y, thr_next.z, rr_next);
+        qout.rad[slot] = make_float4(rad.x, rad.y, rad.z, alpha);
+        qout.meta[slot] = make_uint4(ps_next, job, uint32_t(g), uint32_t(g >> 32));
+        target = qout.rad + slot;
+      } else {
+        J->result[g] = make_float4(rad.x, rad.y, rad.z, alpha);
+        target = J->result + g;
+      }
+    }
+    // Count finished paths per job, one atomic per group of lanes sharing a job.
+    {
+      const bool fin = active && !cont;
+      const uint32_t key = fin ? job : 0xffffffffu;
+      const unsigned m = __match_any_sync(0xffffffffu, key);
+      if (fin && lane == uint32_t(__ffs(m) - 1)) atomicAdd(job_done + job, (unsigned long long)__popc(m));
+    }
+
+    // ---- direct lighting (render/direct-illum.cc:83-255) ----------------
+    // The light loop bound is the largest in the warp, so shadow-ray appends
+    // stay warp-synchronous.
+    uint32_t nl = (alive && J->jc.direct_samples) ? s->n_lights : 0u;
+    uint32_t ns = alive ? J->jc.direct_samples : 0u;
+    for (int off = 16; off > 0; off >>= 1) {
+      nl = max(nl, __shfl_xor_sync(0xffffffffu, nl, off));
+      ns = max(ns, __shfl_xor_sync(0xffffffffu, ns, off));
+    }
+    for (uint32_t l = 0; l < nl; l++) {
+      for (uint32_t jn = 0; jn < ns; jn++) {
+        bool emit_l = false, emit_b = false;
+        float3 c_l = f3(0, 0, 0), c_b = f3(0, 0, 0), dir_l = c_l, dir_b = c_l;
+        float dist_l = 0.f, dist_b = 0.f;
+        const JobConsts &jc = J->jc;
+        if (alive && l < s->n_lights && jn < jc.direct_samples) {
+          const DevLight &L = s->lights[l];
+          const bool point = is_point_light(L);
+          const uint32_t flags = B_ALL & ~B_SPECULAR;
+          const float inv_ns = 1.f / float(jc.direct_samples);
+          const uint32_t kl = K_LIGHT0 + 3 * l;
+          float2 pl, pb;
+          if (bounce < jc.min_len) {
+            const Strata st_direct = strata_for(jc.S * jc.direct_samples);
+            pl = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl));
+            pb = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl + 1));
+          } else {
+            const Strata st_rand = strata_for(jc.direct_samples);
+            pl = strat_uv(st_rand, rng, uint32_t(rng.path_lo ^ (bounce << 24)), jn, dim_of(bounce, kl));
+            pb = strat_uv(st_rand, rng, uint32_t(rng.path_lo ^ (bounce << 24)), jn, dim_of(bounce, kl + 1));
+          }
+          const float extra = rng.u(dim_of(bounce, kl + 2) ^ (jn << 20));
+          LSample ls = light_sample(*s, L, I, pl, extra);
+          if (ls.pdf > 0.f && csum(ls.val) > 0.f) {
+            float bpdf;
+            float3 bv = bsdf_eval(B, I, ls.dir, flags, bpdf);
+            if (csum(bv) > 0.f) {
+              float3 c = ls.val;
+              c = mul3(c, medium_transmittance(med, (ls.dist == 0.f ? jc.horizon : ls.dist) - 2.f * jc.min_trace));
+              if (!point) c = mul(c, mis_weight(ls.pdf, bpdf));
+              c = mul(mul3(c, bv), fabsf(I.cos_n(ls.dir)) / ls.pdf);
+              c_l = mul(mul3(c, thr), inv_ns);
+              dir_l = ls.dir;
+              dist_l = ls.dist;
+              emit_l = true;
+            }
+          }
+          if (!point) {
+            BSample bs = bsdf_sample(B, I, pb, flags);
+            if (bs.pdf > 0.f && csum(bs.val) > 0.f) {
+              LSample lv = light_eval(*s, L, I, bs.dir);
+              if (lv.pdf > 0.f && csum(lv.val) > 0.f) {
+                float3 c = lv.val;
+                c = mul3(c, medium_transmittance(med, (lv.dist == 0.f ? jc.horizon : lv.dist) - 2.f * jc.min_trace));
+                c = mul(c, mis_weight(bs.pdf, lv.pdf));
+                c = mul(mul3(c, bs.val), fabsf(I.cos_n(bs.dir)) / bs.pdf);
+                c_b = mul(mul3(c, thr), inv_ns);
+                dir_b = bs.dir;
+                dist_b = lv.dist;
+                emit_b = true;
+              }
+            }
+          }
+        }
+        uint32_t sl = warp_append(count_sq, emit_l);
+        if (emit_l) {
+          const float3 wd = I.nf.from(dir_l);
+          sq.o[sl] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+          sq.d[sl] = make_float4(wd.x, wd.y, wd.z, (dist_l == 0.f ? jc.horizon : dist_l) - jc.min_trace);
+          sq.c[sl] = make_float4(c_l.x, c_l.y, c_l.z, __uint_as_float(scene));
+          sq.tgt[sl] = reinterpret_cast<unsigned long long>(target);
+        }
+        sl = warp_append(count_sq, emit_b);
+        if (emit_b) {
+          const float3 wd = I.nf.from(dir_b);
+          sq.o[sl] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+          sq.d[sl] = make_float4(wd.x, wd.y, wd.z, (dist_b == 0.f ? jc.horizon : dist_b) - jc.min_trace);
+          sq.c[sl] = make_float4(c_b.x, c_b.y, c_b.z, __uint_as_float(scene));
+          sq.tgt[sl] = reinterpret_cast<unsigned long long>(target);
+        }
+      }
+    }
+  }
+}
+
+template <int STACK>
+void capture_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N,
+                       uint32_t cur, const EngineJobDev *jobs, const DevScene *scenes, EQ qc, EQ qn,
+                       uint32_t *hit_ref, float *hit_t, ESQ sq, unsigned long long *job_done) {
+  const uint32_t sms = uint32_t(num_sms());
+  k_e_plan<<<1, 1, 0, st>>>(ctl, ring, R, N, cur);
+  k_e_regen<<<sms * 8, 256, 0, st>>>(ctl, ring, R, jobs, qc);
+  k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, 128), 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
+                                                                               hit_t);
+  k_e_shade<<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done);
+  k_e_shadow<STACK><<<resident_grid(k_e_shadow<STACK>, 128), 128, 0, st>>>(ctl, scenes, sq);
+}
+
+}  // namespace
+
+Engine::Engine(const EngineConfigHost &cfg) : cfg_(cfg) {
+  t0_ = std::chrono::steady_clock::now();
+  if (cfg_.slots < 1024 || cfg_.item_paths == 0 || cfg_.ring_items < 16 || cfg_.max_jobs == 0 ||
+      cfg_.iters_per_launch == 0)
+    throw Error{SNOG_EINVAL, "engine config out of range"};
+  check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  const size_t N = cfg_.slots, L = cfg_.max_lights ? cfg_.max_lights : 1;
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t o = off;
+    off += (b + 255) & ~size_t(255);
+    return o;
+  };
+  size_t o_q[2][5];
+  for (int k = 0; k < 2; k++)
+    for (int a = 0; a < 5; a++) o_q[k][a] = take(16 * N);
+  size_t o_href = take(4 * N), o_ht = take(4 * N);
+  size_t o_so = take(16 * N * 2 * L), o_sd = take(16 * N * 2 * L), o_sc = take(16 * N * 2 * L),
+         o_st = take(8 * N * 2 * L);
+  size_t o_ctl = take(sizeof(EngineCtl)), o_ring = take(sizeof(WorkItem) * cfg_.ring_items);
+  size_t o_jobs = take(sizeof(EngineJobDev) * cfg_.max_jobs), o_done = take(8 * size_t(cfg_.max_jobs));
+  size_t o_sc2 = take(sizeof(DevScene) * max_scenes_);
+  check_cuda(cudaMalloc(&block_, off), "engine buffers");
+  char *b = static_cast<char *>(block_);
+  for (int k = 0; k < 2; k++) {
+    q_o_[k] = reinterpret_cast<float4 *>(b + o_q[k][0]);
+    q_d_[k] = reinterpret_cast<float4 *>(b + o_q[k][1]);
+    q_thr_[k] = reinterpret_cast<float4 *>(b + o_q[k][2]);
+    q_rad_[k] = reinterpret_cast<float4 *>(b + o_q[k][3]);
+    q_meta_[k] = reinterpret_cast<uint4 *>(b + o_q[k][4]);
+  }
+  hit_ref_ = reinterpret_cast<uint32_t *>(b + o_href);
+  hit_t_ = reinterpret_cast<float *>(b + o_ht);
+  s_o_ = reinterpret_cast<float4 *>(b + o_so);
+  s_d_ = reinterpret_cast<float4 *>(b + o_sd);
+  s_c_ = reinterpret_cast<float4 *>(b + o_sc);
+  s_tgt_ = reinterpret_cast<unsigned long long *>(b + o_st);
+  ctl_ = reinterpret_cast<EngineCtl *>(b + o_ctl);
+  ring_ = reinterpret_cast<WorkItem *>(b + o_ring);
+  jobs_dev_ = reinterpret_cast<EngineJobDev *>(b + o_jobs);
+  job_done_ = reinterpret_cast<unsigned long long *>(b + o_done);
+  scenes_dev_ = reinterpret_cast<DevScene *>(b + o_sc2);
+  check_cuda(cudaMemsetAsync(ctl_, 0, sizeof(EngineCtl), stream_), "memset");
+  check_cuda(cudaMemsetAsync(job_done_, 0, 8 * size_t(cfg_.max_jobs), stream_), "memset");
+  check_cuda(cudaMallocHost(&ctl_host_, sizeof(EngineCtl)), "pinned");
+  check_cuda(cudaMallocHost(&done_host_, 8 * size_t(cfg_.max_jobs)), "pinned");
+  std::memset(done_host_, 0, 8 * size_t(cfg_.max_jobs));
+  for (uint32_t k = cfg_.max_jobs; k > 0; k--) free_slots_.push_back(k - 1);
+  check_cuda(cudaStreamSynchronize(stream_), "engine init");
+}
+
+Engine::~Engine() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto &kv : jobs_) release_job(kv.second);
+  if (graph_) cudaGraphExecDestroy(graph_);
+  cudaFree(block_);
+  cudaFreeHost(ctl_host_);
+  cudaFreeHost(done_host_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+double Engine::now_ms() const {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
+}
+
+uint32_t Engine::add_scene(SceneImpl *scene) {
+  if (!scene->on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
+  if (scenes_.size() >= max_scenes_) throw Error{SNOG_EINVAL, "engine scene table full"};
+  if (!stack_class_for_depth(scene->dev.max_depth))
+    throw Error{SNOG_EINVAL, "octree deeper than the traversal kernels support"};
+  if (scene->dev.n_lights > cfg_.max_lights)
+    throw Error{SNOG_EINVAL, "scene has more lights than the engine's max_lights"};
+  const uint32_t slot = uint32_t(scenes_.size());
+  scenes_.push_back(scene);
+  check_cuda(cudaMemcpyAsync(scenes_dev_ + slot, &scene->dev, sizeof(DevScene), cudaMemcpyHostToDevice, stream_),
+             "scene table");
+  check_cuda(cudaStreamSynchronize(stream_), "scene table");
+  const int sc = stack_class_for_depth(scene->dev.max_depth);
+  if (sc > graph_stack_) {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    graph_stack_ = sc;
+  }
+  return slot;
+}
+
+void Engine::build_graph() {
+  EQ q[2];
+  for (int k = 0; k < 2; k++) q[k] = EQ{q_o_[k], q_d_[k], q_thr_[k], q_rad_[k], q_meta_[k]};
+  ESQ sq{s_o_, s_d_, s_c_, s_tgt_};
+  cudaGraph_t g;
+  check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+  for (uint32_t it = 0; it < cfg_.iters_per_launch; it++) {
+    for (uint32_t cur = 0; cur < 2; cur++) {
+      switch (graph_stack_) {
+        case 32: capture_iteration<32>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
+        case 64: capture_iteration<64>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
+        case 128: capture_iteration<128>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
+        default: capture_iteration<256>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
+      }
+    }
+  }
+  cudaError_t e = cudaStreamEndCapture(stream_, &g);
+  check_cuda(e, "end capture");
+  e = cudaGraphInstantiate(&graph_, g, 0);
+  cudaGraphDestroy(g);
+  check_cuda(e, "graph instantiate");
+}
+
+uint64_t Engine::submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRenderParams &p, float *out,
+                        bool out_on_device, double submit_ms) {
+  if (scene_slot >= scenes_.size()) throw Error{SNOG_ENOTFOUND, "unknown scene slot"};
+  if (p.width == 0 || p.height == 0 || p.spp == 0) throw Error{SNOG_EINVAL, "width, height, spp must be > 0"};
+  if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};
+  if (p.direct_samples > 64) throw Error{SNOG_EINVAL, "direct_samples must be <= 64"};
+  if (uint64_t(p.width + 4) * (p.height + 4) * p.spp >= (1ull << 32))
+    throw Error{SNOG_EINVAL, "a job is limited to 2^32 paths"};
+  if (scenes_[scene_slot]->dev.n_lights * p.direct_samples > cfg_.max_lights)
+    throw Error{SNOG_EINVAL, "lights x direct_samples exceeds the engine's max_lights"};
+  HostJob j;
+  j.id = next_id_++;
+  j.scene_slot = scene_slot;
+  j.jc = make_job(scenes_[scene_slot]->dev, cam, p);
+  j.total = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
+  j.npix = size_t(p.width) * p.height;
+  j.out = out;
+  j.out_on_device = out_on_device;
+  j.bytes = j.total * 24 + j.npix * (20 + (out_on_device ? 0 : 12)) + 4096;
+  if (j.bytes > cfg_.mem_budget) throw Error{SNOG_ENOMEM, "job larger than the engine's memory budget"};
+  j.st.submit_ms = submit_ms >= 0 ? submit_ms : now_ms();
+  j.st.paths = uint64_t(p.width) * p.height * p.spp;
+  const uint64_t id = j.id;
+  jobs_.emplace(id, j);
+  pending_.push_back(id);
+  return id;
+}
+
+bool Engine::cancel(uint64_t id) {
+  auto it = jobs_.find(id);
+  if (it == jobs_.end()) return false;
+  it->second.canceled = true;
+  return true;
+}
+
+void Engine::release_job(HostJob &j) {
+  cudaFree(j.result);
+  cudaFree(j.jit);
+  cudaFree(j.accum);
+  cudaFree(j.wsum);
+  if (!j.out_on_device) cudaFree(j.dev_out);
+  j.result = nullptr;
+  j.jit = nullptr;
+  j.accum = nullptr;
+  j.wsum = nullptr;
+  j.dev_out = nullptr;
+}
+
+// Admit pending jobs in arrival order while the memory budget and the job
+// table allow.
+void Engine::admit() {
+  while (!pending_.empty()) {
+    HostJob &j = jobs_.at(pending_.front());
+    if (j.canceled) {
+      j.st.status = SNOG_ECANCELED;
+      finished_[j.id] = j.st;
+      jobs_.erase(j.id);
+      pending_.pop_front();
+      continue;
+    }
+    if (free_slots_.empty() || budget_used_ + j.bytes > cfg_.mem_budget) break;
+    auto alloc = [&](void **p, size_t n) {
+      cudaError_t e = cudaMalloc(p, n);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      return true;
+    };
+    bool ok = alloc(reinterpret_cast<void **>(&j.result), j.total * 16) &&
+              alloc(reinterpret_cast<void **>(&j.jit), j.total * 8) &&
+              alloc(reinterpret_cast<void **>(&j.accum), j.npix * 16) &&
+              alloc(reinterpret_cast<void **>(&j.wsum), j.npix * 4);
+    if (ok && !j.out_on_device) ok = alloc(reinterpret_cast<void **>(&j.dev_out), j.npix * 12);
+    if (!ok) {
+      release_job(j);
+      if (!active_.empty()) break;   // device full: retry once running jobs have freed memory
+      // Nothing running will free memory: this job cannot be admitted.
+      j.st.status = SNOG_ENOMEM;
+      j.st.finish_ms = now_ms();
+      finished_[j.id] = j.st;
+      jobs_.erase(j.id);
+      pending_.pop_front();
+      continue;
+    }
+    if (j.out_on_device) j.dev_out = j.out;
+    j.table_slot = free_slots_.back();
+    free_slots_.pop_back();
+    budget_used_ += j.bytes;
+    EngineJobDev rec;
+    std::memset(&rec, 0, sizeof rec);
+    rec.jc = j.jc;
+    rec.scene = j.scene_slot;
+    rec.total = j.total;
+    rec.result = j.result;
+    rec.jit = j.jit;
+    check_cuda(cudaMemcpyAsync(jobs_dev_ + j.table_slot, &rec, sizeof rec, cudaMemcpyHostToDevice, stream_),
+               "job record");
+    check_cuda(cudaMemsetAsync(job_done_ + j.table_slot, 0, 8, stream_), "job counter");
+    done_host_[j.table_slot] = 0;
+    j.st.admit_ms = now_ms();
+    active_.push_back(j.id);
+    pending_.pop_front();
+  }
+}
+
+// Push work items round-robin across the active jobs while the ring has room.
+void Engine::push_items() {
+  const uint64_t R = cfg_.ring_items;
+  std::vector<WorkItem> batch;
+  const uint64_t head = last_ctl_.item_head;
+  while (pushed_tail_ + batch.size() - head < R - 1) {
+    bool any = false;
+    for (size_t k = 0; k < active_.size() && pushed_tail_ + batch.size() - head < R - 1; k++) {
+      HostJob &j = jobs_.at(active_[(rr_ + k) % active_.size()]);
+      if (j.canceled || j.pushed >= j.total) continue;
+      WorkItem w;
+      w.job = j.table_slot;
+      w.pad = 0;
+      w.begin = j.pushed;
+      w.count = std::min<uint64_t>(cfg_.item_paths, j.total - j.pushed);
+      w.cum = pushed_cum_;
+      pushed_cum_ += w.count;
+      j.pushed += w.count;
+      if (j.st.start_ms == 0) j.st.start_ms = now_ms();
+      batch.push_back(w);
+      any = true;
+    }
+    if (!any) break;
+    rr_++;
+  }
+  if (batch.empty()) return;
+  // Copy into the ring (possibly wrapping), then publish tail and avail_end.
+  uint64_t pos = pushed_tail_;
+  size_t k = 0;
+  while (k < batch.size()) {
+    const uint64_t slot = pos % R;
+    const size_t run = std::min<size_t>(batch.size() - k, size_t(R - slot));
+    check_cuda(cudaMemcpyAsync(ring_ + slot, batch.data() + k, run * sizeof(WorkItem), cudaMemcpyHostToDevice,
+                               stream_),
+               "ring push");
+    k += run;
+    pos += run;
+  }
+  pushed_tail_ = pos;
+  // tail and avail_end are adjacent fields of the control block
+  unsigned long long pub[2] = {pushed_tail_, pushed_cum_};
+  check_cuda(cudaMemcpyAsync(&ctl_->item_tail, pub, sizeof pub, cudaMemcpyHostToDevice, stream_), "ring tail");
+  check_cuda(cudaStreamSynchronize(stream_), "ring push");   // pub is on the stack
+}
+
+void Engine::finish_job(HostJob &j) {
+  cudaError_t e = splat_job(j.jc, j.result, j.jit, j.total, j.accum, j.wsum, j.dev_out, stream_);
+  check_cuda(e, "splat");
+  kernel_launches_ += 2;
+  if (!j.out_on_device)
+    check_cuda(cudaMemcpyAsync(j.out, j.dev_out, j.npix * 12, cudaMemcpyDeviceToHost, stream_), "image D2H");
+  check_cuda(cudaStreamSynchronize(stream_), "finish");
+  j.st.finish_ms = now_ms();
+  j.st.status = SNOG_OK;
+}
+
+bool Engine::step() {
+  admit();
+  push_items();
+  // After a launch (an even number of iterations) the live rays are in queue 0.
+  const bool inflight = last_ctl_.qcount[0] > 0 || last_ctl_.ticket < pushed_cum_;
+  if (!inflight && active_.empty() && pending_.empty()) return false;
+  if (inflight || !active_.empty()) {
+    if (!graph_) build_graph();
+    check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+    kernel_launches_ += 5 * 2 * cfg_.iters_per_launch;
+    check_cuda(cudaMemcpyAsync(ctl_host_, ctl_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_), "ctl");
+    check_cuda(cudaMemcpyAsync(done_host_, job_done_, 8 * size_t(cfg_.max_jobs), cudaMemcpyDeviceToHost, stream_),
+               "done");
+    check_cuda(cudaStreamSynchronize(stream_), "iteration");
+    last_ctl_ = *ctl_host_;
+    if (last_ctl_.err) throw Error{SNOG_EINVAL, "traversal stack overflow (non-finite ray?)"};
+  }
+  // Completed (or cancelled and drained) jobs.
+  for (size_t k = 0; k < active_.size();) {
+    HostJob &j = jobs_.at(active_[k]);
+    const uint64_t done = done_host_[j.table_slot];
+    const bool drained = done >= j.pushed;
+    if ((done >= j.total) || (j.canceled && drained)) {
+      if (!j.canceled) finish_job(j);
+      else j.st.status = SNOG_ECANCELED, j.st.finish_ms = now_ms();
+      budget_used_ -= j.bytes;
+      release_job(j);
+      free_slots_.push_back(j.table_slot);
+      finished_[j.id] = j.st;
+      jobs_.erase(j.id);
+      active_.erase(active_.begin() + long(k));
+      continue;
+    }
+    k++;
+  }
+  return true;
+}
+
+void Engine::run_to_completion() {
+  while (step()) {
+  }
+}
+
+JobStatsHost Engine::stats(uint64_t id) {
+  auto f = finished_.find(id);
+  if (f != finished_.end()) return f->second;
+  auto j = jobs_.find(id);
+  if (j != jobs_.end()) return j->second.st;
+  JobStatsHost none;
+  none.status = SNOG_ENOTFOUND;
+  return none;
+}
+
+}  // namespace snog

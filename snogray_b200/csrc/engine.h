@@ -1,0 +1,175 @@
+// engine.h -- the streaming render engine: many jobs (scene, camera, image
+// size, samples) traced together by one persistent wavefront with path
+// regeneration, fed by a device work ring of (job, path-range) items.
+//
+// Per iteration (captured once in a CUDA graph, replayed K times per launch):
+//   k_e_plan     one thread: how many queue slots are free, how many paths
+//                the ring still offers; reserves that many path tickets
+//   k_e_regen    new camera paths for the free slots, from the ring items
+//   k_e_closest  octree closest hit for every queued ray (any scene)
+//   k_e_shade    emission, direct lighting (shadow rays), BSDF continuation
+//                and roulette; surviving paths go to the other queue,
+//                finished ones write their radiance to their job's result
+//   k_e_shadow   any-hit for the shadow rays; unoccluded ones add their
+//                contribution to the path's next-queue entry or result
+// The host admits jobs (device-memory budget), pushes their items into the
+// ring round-robin across jobs (so jobs that arrive later interleave with
+// running ones), launches the graph, and gathers-and-filters each job's
+// samples into its image once all its paths are done.
+
+#ifndef SNOG_ENGINE_H
+#define SNOG_ENGINE_H
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/snogray_b200.h"
+#include "scene.h"
+#include "wavefront.h"
+
+namespace snog {
+
+// Device-side job record.
+struct EngineJobDev {
+  JobConsts jc;
+  uint32_t scene;          // index into the engine's scene table
+  uint32_t pad;
+  unsigned long long total;
+  float4 *result;          // per path: radiance rgb, alpha
+  float2 *jit;             // per path: camera jitter in the pixel
+};
+
+// One work item: paths [begin, begin + count) of a job; `cum` is the number of
+// paths of all items pushed before it (tickets are global over the ring).
+struct WorkItem {
+  uint32_t job, pad;
+  unsigned long long begin, count, cum;
+};
+
+// Engine control block (device).
+struct EngineCtl {
+  uint32_t qcount[2];      // live rays in each queue
+  uint32_t scount;         // shadow rays queued this iteration
+  uint32_t err;            // traversal stack overflow
+  uint32_t disp_closest, disp_shadow;
+  uint32_t regen_n, regen_base;
+  unsigned long long ticket;       // next path ticket
+  unsigned long long regen_start;
+  unsigned long long item_head;    // first ring item not fully consumed
+  unsigned long long item_tail;    // one past the last pushed item (host-written)
+  unsigned long long avail_end;    // cum + count of the last pushed item (host-written)
+  unsigned long long rays_closest, rays_shadow, paths_started;
+};
+
+struct EngineConfigHost {
+  uint32_t slots = 1u << 24;       // paths in flight
+  uint32_t item_paths = 1u << 16;  // paths per work item
+  uint32_t ring_items = 1u << 14;
+  uint32_t max_jobs = 4096;
+  uint32_t max_lights = 4;         // light samples per vertex the shadow queue holds
+  uint32_t iters_per_launch = 4;
+  uint64_t mem_budget = 120ull << 30;
+};
+
+struct JobStatsHost {
+  double submit_ms = 0, admit_ms = 0, start_ms = 0, finish_ms = 0;   // since engine start
+  uint64_t paths = 0;
+  int status = SNOG_EBUSY;         // SNOG_OK done, SNOG_EBUSY pending, SNOG_ECANCELED
+};
+
+class Engine {
+ public:
+  explicit Engine(const EngineConfigHost &cfg);
+  ~Engine();
+
+  uint32_t add_scene(SceneImpl *scene);                 // returns slot; throws
+  // Queue a job; OUT is a host (on_device = false) or device image buffer.
+  // SUBMIT_MS (engine clock) overrides the submission time recorded.
+  uint64_t submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRenderParams &p, float *out,
+                  bool out_on_device, double submit_ms = -1);
+  bool cancel(uint64_t job);
+  // Drive the engine until every submitted job is finished (batch mode).
+  void run_to_completion();
+  // One scheduling round: admit, push items, one graph launch, completions.
+  // Returns false when there is nothing in flight and nothing pending.
+  bool step();
+  JobStatsHost stats(uint64_t job);
+  uint64_t rays_closest() const { return last_ctl_.rays_closest; }
+  uint64_t rays_shadow() const { return last_ctl_.rays_shadow; }
+  double now_ms() const;
+  uint32_t launches() const { return kernel_launches_; }
+
+  std::mutex mu;   // guards the host job tables (server threads)
+
+ private:
+  struct HostJob {
+    uint64_t id;
+    uint32_t scene_slot, table_slot = ~0u;
+    JobConsts jc;
+    uint64_t total, pushed = 0;
+    size_t npix;
+    float *out;
+    bool out_on_device;
+    float4 *result = nullptr;
+    float2 *jit = nullptr;
+    float4 *accum = nullptr;
+    float *wsum = nullptr;
+    float *dev_out = nullptr;
+    uint64_t bytes = 0;
+    bool canceled = false;
+    JobStatsHost st;
+  };
+
+  void build_graph();
+  void admit();
+  void push_items();
+  void finish_job(HostJob &j);
+  void release_job(HostJob &j);
+
+  EngineConfigHost cfg_;
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t graph_ = nullptr;
+  int graph_stack_ = 0;
+  // device buffers
+  void *block_ = nullptr;
+  float4 *q_o_[2], *q_d_[2], *q_thr_[2], *q_rad_[2];
+  uint4 *q_meta_[2];
+  uint32_t *hit_ref_;
+  float *hit_t_;
+  float4 *s_o_, *s_d_, *s_c_;
+  unsigned long long *s_tgt_;
+  EngineCtl *ctl_;
+  WorkItem *ring_;
+  EngineJobDev *jobs_dev_;
+  unsigned long long *job_done_;
+  DevScene *scenes_dev_;
+  uint32_t max_scenes_ = 64;
+  // host mirrors
+  EngineCtl *ctl_host_ = nullptr;              // pinned
+  unsigned long long *done_host_ = nullptr;    // pinned
+  EngineCtl last_ctl_{};
+  std::vector<SceneImpl *> scenes_;
+  std::vector<uint32_t> free_slots_;
+  std::deque<uint64_t> pending_;
+  std::vector<uint64_t> active_;
+  std::map<uint64_t, HostJob> jobs_;
+  std::map<uint64_t, JobStatsHost> finished_;
+  uint64_t next_id_ = 1;
+  uint64_t pushed_tail_ = 0, pushed_cum_ = 0;
+  uint64_t budget_used_ = 0;
+  size_t rr_ = 0;
+  uint32_t kernel_launches_ = 0;
+  std::chrono::steady_clock::time_point t0_;
+};
+
+}  // namespace snog
+
+#endif

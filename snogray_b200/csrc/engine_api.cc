@@ -1,0 +1,336 @@
+// engine_api.cc -- extern "C" entry points for batched and served rendering
+// (include/snogray_b200.h): snog_render_batch drives the streaming engine to
+// completion on the calling thread; a SnogServer runs it on a background
+// thread and accepts jobs at any time.
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "engine.h"
+
+namespace snog {
+int set_error(int code, const std::string &msg);
+extern thread_local std::string g_last_error;
+}  // namespace snog
+
+using namespace snog;
+
+namespace {
+
+template <class F>
+int api_call(F &&f) {
+  try {
+    g_last_error.clear();
+    return f();
+  } catch (const Error &e) {
+    return set_error(e.code, e.msg);
+  } catch (const std::bad_alloc &) {
+    return set_error(SNOG_ENOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return set_error(SNOG_EINVAL, e.what());
+  }
+}
+
+EngineConfigHost to_host(const SnogEngineConfig *c) {
+  EngineConfigHost h;
+  if (!c) return h;
+  h.slots = c->slots;
+  h.item_paths = c->item_paths;
+  h.ring_items = c->ring_items;
+  h.max_jobs = c->max_jobs;
+  h.max_lights = c->max_lights;
+  h.iters_per_launch = c->iters_per_launch;
+  h.mem_budget = c->mem_budget;
+  return h;
+}
+
+void fill(SnogJobStats *o, const JobStatsHost &s) {
+  o->submit_ms = s.submit_ms;
+  o->admit_ms = s.admit_ms;
+  o->start_ms = s.start_ms;
+  o->finish_ms = s.finish_ms;
+  o->paths = s.paths;
+  o->status = s.status;
+}
+
+}  // namespace
+
+struct SnogServer {
+  std::unique_ptr<Engine> engine;
+  std::mutex engine_mu;                 // held while the engine is driven
+  std::mutex mu;                        // inbox, results
+  std::condition_variable cv_work, cv_done;
+  std::thread worker;
+  bool stop = false;
+  std::string thread_error;
+  struct Inbox {
+    uint64_t id;
+    uint32_t slot;
+    SnogCamera cam;
+    SnogRenderParams p;
+    float *out;
+    double submit_ms;
+  };
+  std::deque<Inbox> inbox;
+  std::vector<uint64_t> cancels;
+  std::unordered_map<uint64_t, uint64_t> to_engine;   // server id -> engine id
+  std::map<uint64_t, JobStatsHost> results;           // finished
+  std::map<uint64_t, std::string> failed;             // refused at admission
+  uint64_t next_id = 1;
+
+  void run() {
+    for (;;) {
+      std::vector<Inbox> take;
+      std::vector<uint64_t> cancel_now;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return stop || !inbox.empty() || !to_engine.empty() || !cancels.empty(); });
+        if (stop) return;
+        take.assign(inbox.begin(), inbox.end());
+        inbox.clear();
+        cancel_now.swap(cancels);
+      }
+      std::vector<std::pair<uint64_t, JobStatsHost>> finished;
+      try {
+        std::lock_guard<std::mutex> elk(engine_mu);
+        for (auto &in : take) {
+          try {
+            uint64_t eid = engine->submit(in.slot, in.cam, in.p, in.out, false, in.submit_ms);
+            std::lock_guard<std::mutex> lk(mu);
+            to_engine[in.id] = eid;
+          } catch (const Error &e) {
+            std::lock_guard<std::mutex> lk(mu);
+            failed[in.id] = e.msg;
+          }
+        }
+        for (uint64_t id : cancel_now) {
+          std::lock_guard<std::mutex> lk(mu);
+          auto it = to_engine.find(id);
+          if (it != to_engine.end()) engine->cancel(it->second);
+        }
+        engine->step();
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto it = to_engine.begin(); it != to_engine.end();) {
+          JobStatsHost s = engine->stats(it->second);
+          if (s.status != SNOG_EBUSY) {
+            finished.push_back({it->first, s});
+            it = to_engine.erase(it);
+          } else {
+            ++it;
+          }
+        }
+      } catch (const std::exception &e) {
+        std::lock_guard<std::mutex> lk(mu);
+        thread_error = e.what();
+        for (auto &kv : to_engine) failed[kv.first] = thread_error;
+        to_engine.clear();
+      } catch (const Error &e) {
+        std::lock_guard<std::mutex> lk(mu);
+        thread_error = e.msg;
+        for (auto &kv : to_engine) failed[kv.first] = thread_error;
+        to_engine.clear();
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto &f : finished) results[f.first] = f.second;
+      }
+      cv_done.notify_all();
+    }
+  }
+};
+
+extern "C" {
+
+int snog_engine_default_config(SnogEngineConfig *cfg) {
+  return api_call([&] {
+    if (!cfg) throw Error{SNOG_EINVAL, "null argument"};
+    EngineConfigHost h;
+    cfg->slots = h.slots;
+    cfg->item_paths = h.item_paths;
+    cfg->ring_items = h.ring_items;
+    cfg->max_jobs = h.max_jobs;
+    cfg->max_lights = h.max_lights;
+    cfg->iters_per_launch = h.iters_per_launch;
+    cfg->mem_budget = h.mem_budget;
+    return int(SNOG_OK);
+  });
+}
+
+int snog_render_batch(SnogScene *const *scenes, const SnogCamera *cameras, const SnogRenderParams *params,
+                      uint32_t n_jobs, float *const *outs, int outs_on_device, const SnogEngineConfig *cfg,
+                      SnogBatchStats *stats) {
+  return api_call([&] {
+    if (n_jobs && (!scenes || !cameras || !params || !outs)) throw Error{SNOG_EINVAL, "null argument"};
+    EngineConfigHost h = to_host(cfg);
+    if (!cfg) {
+      // Size the ray queues to the batch: no more slots than paths.
+      uint64_t total = 0;
+      for (uint32_t i = 0; i < n_jobs; i++)
+        total += uint64_t(params[i].width + 4) * (params[i].height + 4) * params[i].spp;
+      while (h.slots > 65536 && uint64_t(h.slots) / 2 >= total) h.slots /= 2;
+      uint32_t ml = 1;
+      for (uint32_t i = 0; i < n_jobs; i++) {
+        if (!scenes[i]) throw Error{SNOG_EINVAL, "null scene"};
+        ml = std::max(ml, scenes[i]->impl->dev.n_lights * std::max(1u, params[i].direct_samples));
+      }
+      h.max_lights = ml;
+      if (h.max_jobs < n_jobs) h.max_jobs = n_jobs;
+    }
+    Engine eng(h);
+    std::unordered_map<SceneImpl *, uint32_t> slot_of;
+    for (uint32_t i = 0; i < n_jobs; i++) {
+      if (!scenes[i]) throw Error{SNOG_EINVAL, "null scene"};
+      SceneImpl *si = scenes[i]->impl;
+      if (!slot_of.count(si)) slot_of[si] = eng.add_scene(si);
+    }
+    const double t0 = eng.now_ms();
+    uint64_t paths = 0;
+    std::vector<uint64_t> ids(n_jobs);
+    for (uint32_t i = 0; i < n_jobs; i++) {
+      ids[i] = eng.submit(slot_of[scenes[i]->impl], cameras[i], params[i], outs[i], outs_on_device != 0);
+      paths += uint64_t(params[i].width) * params[i].height * params[i].spp;
+    }
+    eng.run_to_completion();
+    for (uint32_t i = 0; i < n_jobs; i++)
+      if (eng.stats(ids[i]).status != SNOG_OK)
+        throw Error{eng.stats(ids[i]).status, "job " + std::to_string(i) + " could not be rendered (device memory)"};
+    if (stats) {
+      stats->paths = paths;
+      stats->closest_rays = eng.rays_closest();
+      stats->shadow_rays = eng.rays_shadow();
+      stats->wall_ms = eng.now_ms() - t0;
+      stats->kernel_launches = eng.launches();
+    }
+    return int(SNOG_OK);
+  });
+}
+
+int snog_server_create(const SnogEngineConfig *cfg, SnogServer **out) {
+  return api_call([&] {
+    if (!out) throw Error{SNOG_EINVAL, "null argument"};
+    std::unique_ptr<SnogServer> s(new SnogServer);
+    s->engine.reset(new Engine(to_host(cfg)));
+    SnogServer *raw = s.get();
+    s->worker = std::thread([raw] { raw->run(); });
+    *out = s.release();
+    return int(SNOG_OK);
+  });
+}
+
+int snog_server_add_scene(SnogServer *server, SnogScene *scene, uint32_t *slot) {
+  return api_call([&] {
+    if (!server || !scene || !slot) throw Error{SNOG_EINVAL, "null argument"};
+    std::lock_guard<std::mutex> elk(server->engine_mu);
+    *slot = server->engine->add_scene(scene->impl);
+    return int(SNOG_OK);
+  });
+}
+
+int snog_server_submit(SnogServer *server, uint32_t slot, const SnogCamera *camera,
+                       const SnogRenderParams *params, float *host_out, uint64_t *job_id) {
+  return api_call([&] {
+    if (!server || !camera || !params || !host_out || !job_id) throw Error{SNOG_EINVAL, "null argument"};
+    {
+      std::lock_guard<std::mutex> lk(server->mu);
+      if (!server->thread_error.empty()) throw Error{SNOG_ECUDA, "server stopped: " + server->thread_error};
+      const uint64_t id = server->next_id++;
+      server->inbox.push_back(SnogServer::Inbox{id, slot, *camera, *params, host_out,
+                                                server->engine->now_ms()});
+      *job_id = id;
+    }
+    server->cv_work.notify_one();
+    return int(SNOG_OK);
+  });
+}
+
+static int server_status(SnogServer *server, uint64_t job_id, SnogJobStats *stats) {
+  auto r = server->results.find(job_id);
+  if (r != server->results.end()) {
+    if (stats) fill(stats, r->second);
+    if (r->second.status == SNOG_OK) return int(SNOG_OK);
+    return set_error(r->second.status, r->second.status == SNOG_ECANCELED ? "job was cancelled"
+                                                                          : "job could not be admitted (device memory)");
+  }
+  auto f = server->failed.find(job_id);
+  if (f != server->failed.end()) return set_error(SNOG_EINVAL, f->second);
+  if (job_id == 0 || job_id >= server->next_id) return set_error(SNOG_ENOTFOUND, "unknown job");
+  return int(SNOG_EBUSY);
+}
+
+int snog_server_poll(SnogServer *server, uint64_t job_id, SnogJobStats *stats) {
+  return api_call([&] {
+    if (!server) throw Error{SNOG_EINVAL, "null argument"};
+    std::lock_guard<std::mutex> lk(server->mu);
+    return server_status(server, job_id, stats);
+  });
+}
+
+int snog_server_wait(SnogServer *server, uint64_t job_id, uint32_t timeout_ms, SnogJobStats *stats) {
+  return api_call([&] {
+    if (!server) throw Error{SNOG_EINVAL, "null argument"};
+    std::unique_lock<std::mutex> lk(server->mu);
+    int rc = server_status(server, job_id, stats);
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+    while (rc == SNOG_EBUSY) {
+      if (server->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
+        rc = server_status(server, job_id, stats);
+        if (rc == SNOG_EBUSY) return set_error(SNOG_ETIMEOUT, "job still running");
+        break;
+      }
+      rc = server_status(server, job_id, stats);
+    }
+    return rc;
+  });
+}
+
+int snog_server_cancel(SnogServer *server, uint64_t job_id) {
+  return api_call([&] {
+    if (!server) throw Error{SNOG_EINVAL, "null argument"};
+    {
+      std::lock_guard<std::mutex> lk(server->mu);
+      for (auto it = server->inbox.begin(); it != server->inbox.end(); ++it)
+        if (it->id == job_id) {
+          JobStatsHost s;
+          s.status = SNOG_ECANCELED;
+          s.submit_ms = it->submit_ms;
+          server->results[job_id] = s;
+          server->inbox.erase(it);
+          return int(SNOG_OK);
+        }
+      if (job_id == 0 || job_id >= server->next_id) return set_error(SNOG_ENOTFOUND, "unknown job");
+      if (server->results.count(job_id) || server->failed.count(job_id)) return int(SNOG_OK);   // already over
+      // Running, or taken by the worker and about to be: the worker applies
+      // cancels after the submissions it has taken.
+      server->cancels.push_back(job_id);
+    }
+    server->cv_work.notify_one();
+    return int(SNOG_OK);
+  });
+}
+
+int snog_server_destroy(SnogServer *server) {
+  return api_call([&] {
+    if (!server) return int(SNOG_OK);
+    {
+      std::lock_guard<std::mutex> lk(server->mu);
+      server->stop = true;
+    }
+    server->cv_work.notify_all();
+    if (server->worker.joinable()) server->worker.join();
+    delete server;
+    return int(SNOG_OK);
+  });
+}
+
+}  // extern "C"

@@ -260,25 +260,27 @@ struct Traversal {
       // then tested in list order.
       const uint4 ids = __ldg(reinterpret_cast<const uint4 *>(s.plist + lp));
       const uint32_t nv = lend - lp < 4u ? lend - lp : 4u;
-      PrimRec r0 = load_prim(s, ids.x), r1, r2, r3;
-      if (nv > 1) r1 = load_prim(s, ids.y);
-      if (nv > 2) r2 = load_prim(s, ids.z);
-      if (nv > 3) r3 = load_prim(s, ids.w);
       lp += 4;
       cnt.tests += nv;
-      if (test_prim(r0, o, d, t0, t1)) {
+      // Two records in flight: the next one is fetched while this one is
+      // tested (keeps live registers, and so occupancy, in check).
+      PrimRec ra = load_prim(s, ids.x);
+      PrimRec rb = load_prim(s, nv > 1 ? ids.y : ids.x);
+      if (test_prim(ra, o, d, t0, t1)) {
         hit_ref = ids.x;
         if (ANY) return true;
       }
-      if (nv > 1 && test_prim(r1, o, d, t0, t1)) {
+      if (nv > 2) ra = load_prim(s, ids.z);
+      if (nv > 1 && test_prim(rb, o, d, t0, t1)) {
         hit_ref = ids.y;
         if (ANY) return true;
       }
-      if (nv > 2 && test_prim(r2, o, d, t0, t1)) {
+      if (nv > 3) rb = load_prim(s, ids.w);
+      if (nv > 2 && test_prim(ra, o, d, t0, t1)) {
         hit_ref = ids.z;
         if (ANY) return true;
       }
-      if (nv > 3 && test_prim(r3, o, d, t0, t1)) {
+      if (nv > 3 && test_prim(rb, o, d, t0, t1)) {
         hit_ref = ids.w;
         if (ANY) return true;
       }

@@ -30,39 +30,12 @@
 #include <cstring>
 
 #include "launch.h"
-#include "shade.cuh"
+#include "pathstate.cuh"
 #include "wavefront.h"
 
 namespace snog {
 
 namespace {
-
-// ---- path state word ------------------------------------------------------
-__device__ __forceinline__ uint32_t ps_len(uint32_t p) { return p & 0xffu; }
-__device__ __forceinline__ bool ps_spec(uint32_t p) { return (p >> 8) & 1u; }
-__device__ __forceinline__ uint32_t ps_depth(uint32_t p) { return (p >> 9) & 3u; }
-__device__ __forceinline__ uint32_t ps_medium(uint32_t p, uint32_t k) { return (p >> (11 + 7 * k)) & 0x7fu; }
-
-// Media::update_stack_for_transmission (material/media.cc:76-118): entering a
-// surface with a medium pushes it, leaving pops (never below the camera's
-// medium).  The stack holds three entries; a fourth push drops the oldest.
-__device__ __forceinline__ uint32_t ps_push(uint32_t p, uint32_t mid) {
-  uint32_t d = ps_depth(p);
-  uint32_t ids[3] = {ps_medium(p, 0), ps_medium(p, 1), ps_medium(p, 2)};
-  if (d == 3) {
-    ids[0] = ids[1];
-    ids[1] = ids[2];
-    d = 2;
-  }
-  ids[d] = mid & 0x7fu;
-  d++;
-  return (p & 0x1ffu) | (d << 9) | (ids[0] << 11) | (ids[1] << 18) | (ids[2] << 25);
-}
-__device__ __forceinline__ uint32_t ps_pop(uint32_t p) {
-  uint32_t d = ps_depth(p);
-  if (d == 0) return p;
-  return (p & ~(3u << 9)) | ((d - 1) << 9);
-}
 
 struct PathPtrs {
   float4 *thr, *rad;
@@ -76,28 +49,6 @@ struct RayQ {
 struct ShadowQ {
   float4 *o, *d, *c;
 };
-
-// RNG dimensions: vertex b, slot k.
-enum : uint32_t { K_CAMERA = 0, K_BSDF = 1, K_RR = 2, K_LIGHT0 = 3 };
-__device__ __forceinline__ uint32_t dim_of(uint32_t b, uint32_t k) { return (b << 12) | k; }
-
-__device__ __forceinline__ Strata strata_for(uint32_t n) {
-  // Grid::adjust_uv_sample_count (render/grid.cc:70-80)
-  double sq = sqrt(double(n));
-  uint32_t up = uint32_t(ceil(sq)), down = uint32_t(floor(sq + 0.5));
-  if (down == 0) down = 1;
-  return Strata{n, up, down, up * down};
-}
-
-__device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred) {
-  const uint32_t lane = threadIdx.x & 31u;
-  unsigned mask = __ballot_sync(0xffffffffu, pred);
-  if (!mask) return 0;
-  uint32_t leader = __ffs(mask) - 1, base = 0;
-  if (lane == leader) base = atomicAdd(counter, uint32_t(__popc(mask)));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return base + uint32_t(__popc(mask & ((1u << lane) - 1u)));
-}
 
 // ---- kernels -----------------------------------------------------------------
 
@@ -221,12 +172,6 @@ __global__ void __launch_bounds__(128, 6) k_trace_shadow(DevScene s, ShadowQ q, 
   }
   if (c.overflow) atomicOr(counters + 3, 1u);
   if (prof) warp_count(stats + 4, c.nodes, c.tests);
-}
-
-__device__ __forceinline__ float3 medium_transmittance(const DevMedium &m, float len) {
-  // Medium::transmittance (material/medium.h:37-40), pow (e, -absorb * d).
-  if (m.absorb[0] == 0.f && m.absorb[1] == 0.f && m.absorb[2] == 0.f) return f3(1.f, 1.f, 1.f);
-  return f3(expf(-m.absorb[0] * len), expf(-m.absorb[1] * len), expf(-m.absorb[2] * len));
 }
 
 __global__ void __launch_bounds__(128) k_shade(DevScene s, JobConsts jc, uint64_t base, uint32_t bounce,
@@ -721,6 +666,22 @@ cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, 
   if (prof) prof->end(st);
   nl++;
   if (launches) *launches += nl;
+  return cudaGetLastError();
+}
+
+}  // namespace snog
+
+namespace snog {
+
+cudaError_t splat_job(const JobConsts &jc, const float4 *rad, const float2 *jit, uint64_t total, float4 *accum,
+                      float *wsum, float *out_rgb, cudaStream_t st) {
+  const uint64_t npix = uint64_t(jc.W) * jc.H;
+  cudaError_t e = cudaMemsetAsync(accum, 0, npix * sizeof(float4), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(wsum, 0, npix * sizeof(float), st);
+  if (e != cudaSuccess) return e;
+  const uint32_t grid256 = uint32_t(num_sms()) * 8;
+  k_splat<<<grid256, 256, 0, st>>>(jc, 0, uint32_t(total), rad, jit, accum, wsum, 0, int(jc.H));
+  k_resolve<<<grid256, 256, 0, st>>>(uint32_t(npix), accum, wsum, out_rgb);
   return cudaGetLastError();
 }
 

@@ -72,6 +72,12 @@ struct RenderProfile {
 // device).  Paths are processed in waves of at most wb.wave_cap.  With PROF,
 // every launch is bracketed by events and the traversal counts its node
 // visits and primitive tests into wb.stats[2..5].
+// Mitchell-filter all TOTAL samples of a finished job (radiance + alpha and
+// camera jitter per path, pattern-pixel-major) into its image: clears
+// accum/wsum, gathers, resolves into out_rgb.
+cudaError_t splat_job(const JobConsts &jc, const float4 *rad, const float2 *jit, uint64_t total, float4 *accum,
+                      float *wsum, float *out_rgb, cudaStream_t st);
+
 cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, float4 *accum,
                        float *wsum, float *out_rgb, cudaStream_t st, uint32_t *waves, uint32_t *launches,
                        RenderProfile *prof = nullptr);

@@ -10,12 +10,25 @@ reference's own rate (paths rendered in the filter margin are extra work not
 counted).  Synthetic data: the scene is generated from fixed seeds.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--batch-jobs 1024] [--serve-requests 200] [--serve-rates 100]
 
-`value` is device time (CUDA events on the render stream, inputs resident in
-HBM); `e2e` is the same metric through the public host API (snog_render: job
-description in from host memory, the finished image copied back to host
-memory every step), wall clock.  The path state and queues of a wave (~1.2 GB)
-exceed the 126 MB L2, so no flush is needed between steps.
+`value` is device time (CUDA events on the engine's stream, inputs resident
+in HBM) of the streaming engine (snog_engine_render, configuration picked by
+snog_engine_autotune); `e2e` is the same metric through the public C ABI with
+the image copied back into pinned host memory every step, wall clock;
+`plain` is the drop-in renderer (snog_render_device: one job, its own launch
+sequence) on the same job.  The path state and queues (several GB) exceed the
+126 MB L2, so no flush is needed between steps.
+
+Two more workloads run after the headline (rank 0, N=1), each against the
+plain renderer doing one job per launch sequence on the same input:
+`batched` -- 1024 independent random-triangle soups of 1k-50k triangles
+(log-uniform), resolution {64,128,256}^2, spp {4,16,64}, one engine run; and
+`serve` -- 8 resident scenes of 10k-8M triangles, requests at Poisson arrivals
+(random scene, camera, resolution {128..1024}^2, spp {4,16,64}), p50/p95/p99
+latency from arrival to the image in host memory.  The default takes the
+first 200 requests of the stream at 100 requests/s; --serve-requests 2000
+--serve-rates 50,200,1000,2000 runs the full sweep.
 
 Multi-GPU: the path shards trivially (independent paths); each rank renders
 its own job replica (weak scaling), no collective on the data path.  Rank 0
@@ -224,6 +237,142 @@ def bench_isec(args, n_tri=1 << 20, n_rays=1 << 24):
     return out
 
 
+def _cfg_dict(cfg):
+    return {f: getattr(cfg, f) for f, _ in cfg._fields_ if f != "reserved"}
+
+
+def _pct(xs, q):
+    return round(float(np.percentile(np.asarray(xs), q)), 2) if len(xs) else None
+
+
+def read_traffic_per_ray():
+    """DRAM bytes per closest-hit ray of the engine's traversal kernel, from
+    the committed ncu summary (one capture of the same kernel on a smaller
+    terrain render; traffic scales with rays)."""
+    path = os.path.join(HERE, "profiles", "k_e_closest_terrain.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for ln in f:
+            if ln.startswith("dram_bytes_per_ray:"):
+                return float(ln.split(":", 1)[1])
+    return None
+
+
+def bench_batch(args, sb, scenes, torch, stream):
+    """Batched workload: 1024 independent soups of 1k-50k triangles
+    (log-uniform), resolution from {64,128,256}^2, spp from {4,16,64}, all in
+    one engine run, beside the plain renderer doing one job after another."""
+    t0 = time.perf_counter()
+    work = scenes.batch_workload(args.batch_jobs)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    handles = [sb.Scene(sd) for sd, _, _ in work]
+    build_s = time.perf_counter() - t0
+    jobs = [(h, cam, p) for h, (_, cam, p) in zip(handles, work)]
+    paths = sum(p.width * p.height * p.spp for _, _, p in jobs)
+    outs = [torch.empty((p.height, p.width, 3), dtype=torch.float32, device="cuda") for _, _, p in jobs]
+    ptrs = [o.data_ptr() for o in outs]
+    t0 = time.perf_counter()
+    cfg, _ = sb.autotune(jobs, sample_jobs=64)
+    tune_s = time.perf_counter() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with sb.Engine(cfg, stream=stream.cuda_stream) as eng:
+        eng.render(jobs, device_outs=ptrs)        # warm: graph, job-buffer cache
+        torch.cuda.synchronize()
+        e0.record(stream)
+        _, st = eng.render(jobs, device_outs=ptrs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    eng_ms = e0.elapsed_time(e1)
+    # plain: one render call per job, in order, same stream
+    plain_outs = [torch.empty_like(o) for o in outs]
+    for k in range(min(3, len(jobs))):       # pool and kernels warm
+        jobs[k][0].render_device(jobs[k][1], jobs[k][2], plain_outs[k].data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for (h, cam, p), o in zip(jobs, plain_outs):
+        h.render_device(cam, p, o.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    n_off = sum(not torch.allclose(a, b, rtol=1e-4, atol=1e-5) for a, b in zip(outs, plain_outs))
+    worst = max(float(((a - b).abs() / (b.abs() + 1e-3)).max()) for a, b in zip(outs, plain_outs))
+    for h in handles:
+        h.close()
+    return {"workload": f"{len(jobs)} random-triangle soups (1k-50k tris, log-uniform), "
+                        "res {64,128,256}^2, spp {4,16,64}, one area light each",
+            "paths": paths, "triangles": int(sum(len(sd.triangles) for sd, _, _ in work)),
+            "engine_mpaths_per_s": round(paths / eng_ms * 1e-3, 2),
+            "plain_mpaths_per_s": round(paths / plain_ms * 1e-3, 2),
+            "speedup_vs_plain": round(plain_ms / eng_ms, 3),
+            "engine_ms": round(eng_ms, 1), "plain_ms": round(plain_ms, 1),
+            "engine_mrays_per_s": round((st["closest_rays"] + st["shadow_rays"]) / eng_ms * 1e-3, 2),
+            "images_vs_plain": {"jobs_outside_rtol_1e-4": int(n_off),
+                                "max_rel_diff": round(worst, 6)},
+            "autotuned": _cfg_dict(cfg),
+            "setup_s": {"generate": round(gen_s, 1), "octree_build_upload": round(build_s, 1),
+                        "autotune": round(tune_s, 1)}}
+
+
+def bench_serve(args, sb, scenes):
+    """Serving workload: 8 resident soups (10k-8M triangles), requests at
+    Poisson arrivals, each a random scene / camera / resolution / spp.  The
+    server (continuous batching) and the plain renderer (one job per launch,
+    first come first served) get the same request stream; latency is arrival
+    to result in host memory."""
+    import threading
+    t0 = time.perf_counter()
+    sds = scenes.serve_scenes()
+    handles = [sb.Scene(sd) for sd in sds]
+    setup_s = time.perf_counter() - t0
+    out = {"workload": "8 resident random-triangle scenes (10k,50k,200k,1M,2M,4M,6M,8M tris; "
+                       "area light or sky envmap), Poisson arrivals, res {128,256,512,1024}^2, "
+                       "spp {4,16,64}, 120 GB admission budget",
+           "requests": args.serve_requests, "setup_s": round(setup_s, 1), "rates": []}
+    # warm the plain path and the kernels once per scene
+    for h in handles:
+        h.render(scenes.orbit_camera(32, 32, np.random.default_rng(0)), sb.RenderParams(32, 32, 1))
+    for rate in args.serve_rates:
+        reqs = scenes.serve_requests(args.serve_requests, rate)
+        paths = sum(r.params.width * r.params.height * r.params.spp for r in reqs)
+        # ---- served: continuous batching --------------------------------
+        cfg = sb.engine_config(max_lights=4, mem_budget=120 << 30)
+        with sb.Server(cfg) as srv:
+            slots = [srv.add_scene(h) for h in handles]
+            ids = []
+            t_start = time.perf_counter()
+            for r in reqs:
+                dt = r.arrival_s - (time.perf_counter() - t_start)
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(slots[r.scene], r.camera, r.params))
+            res = [srv.wait(j, timeout_ms=600000)[1] for j in ids]
+        lat_s = [st["finish_ms"] - st["submit_ms"] for st in res]
+        span_s = (max(st["finish_ms"] for st in res) - min(st["submit_ms"] for st in res)) * 1e-3
+        # ---- plain: one job per launch, FIFO ------------------------------
+        lat_p = []
+        lock = threading.Lock()
+        t_start = time.perf_counter()
+        for r in reqs:
+            now = time.perf_counter() - t_start
+            if now < r.arrival_s:
+                time.sleep(r.arrival_s - now)
+            handles[r.scene].render(r.camera, r.params)
+            with lock:
+                lat_p.append((time.perf_counter() - t_start - r.arrival_s) * 1e3)
+        span_p = time.perf_counter() - t_start
+        out["rates"].append({
+            "rate_req_per_s": rate, "paths": paths,
+            "served": {"p50_ms": _pct(lat_s, 50), "p95_ms": _pct(lat_s, 95), "p99_ms": _pct(lat_s, 99),
+                       "mpaths_per_s": round(paths / span_s * 1e-6, 2), "makespan_s": round(span_s, 2)},
+            "plain": {"p50_ms": _pct(lat_p, 50), "p95_ms": _pct(lat_p, 95), "p99_ms": _pct(lat_p, 99),
+                      "mpaths_per_s": round(paths / span_p * 1e-6, 2), "makespan_s": round(span_p, 2)}})
+    for h in handles:
+        h.close()
+    return out
+
+
 def bench_ours(args):
     import ctypes
 
@@ -240,25 +389,38 @@ def bench_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
-    sd, cam = workload()
-    scene = sb.Scene(sd)
-    params = scenes.terrain_params(WIDTH, HEIGHT, SPP, seed=1 + rank)
-    out = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, device="cuda")
-    stream = torch.cuda.Stream()
-    sptr = stream.cuda_stream
-
-    def step(want_stats=False):
-        return scene.render_device(cam, params, out.data_ptr(), sptr, want_stats=want_stats)
-
     def barrier():
         if pg is not None:
             pg.barrier()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    sd, cam = workload()
+    scene = sb.Scene(sd)
+    params = scenes.terrain_params(WIDTH, HEIGHT, SPP, seed=1 + rank)
+    job = [(scene, cam, params)]
+    out = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    paths_per_step = WIDTH * HEIGHT * SPP
+
+    # ---- engine configuration picked by the autotuner ----------------------
+    cfg, _ = sb.autotune(job, sample_jobs=1)
+    eng = sb.Engine(cfg, stream=sptr)
+
+    def step():
+        return eng.render(job, device_outs=[out.data_ptr()])[1]
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
 
-    # ---- timed region: device time on the render stream ------------------
+    # ---- timed region: device time on the engine's stream ------------------
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -267,45 +429,48 @@ def bench_ours(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     launches = 0
+    rays = [0, 0]
     for _ in range(args.steps):
-        st = step(want_stats=False)
+        st = step()
+        launches += st["kernel_launches"]
+        rays[0] += st["closest_rays"]
+        rays[1] += st["shadow_rays"]
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    paths_per_step = WIDTH * HEIGHT * SPP
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     value = paths_per_step * ws / ms * 1e-3          # Mpaths/s, whole job
+
+    # ---- the plain renderer (one job per launch sequence) on the same job --
+    scene.render_device(cam, params, out.data_ptr(), sptr)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    n_plain = 2
+    for _ in range(n_plain):
+        scene.render_device(cam, params, out.data_ptr(), sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(e0.elapsed_time(e1) / n_plain)
 
     # ---- per-kernel times for the roofline (live, CUDA events) ------------
     os.environ["SNOG_PROFILE_KERNELS"] = "1"
-    prof = step(want_stats=True)
+    prof = step()
     del os.environ["SNOG_PROFILE_KERNELS"]
-    launches = prof["kernel_launches"]
 
-    # ---- e2e through the public host API ----------------------------------
+    # ---- e2e through the public C ABI with host buffers --------------------
     pinned = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, pin_memory=True)
     host = pinned.numpy()
     barrier()
     t0 = time.perf_counter()
     n_e2e = max(1, args.steps)
     for _ in range(n_e2e):
-        cs, ps = sb.camera_struct(cam), sb.params_struct(params)
-        stt = sb.SnogRenderStats()
-        sb._check(sb._render(scene.handle, ctypes.byref(cs), ctypes.byref(ps), host.ctypes.data,
-                             ctypes.byref(stt)))
-    e2e_s = (time.perf_counter() - t0) / n_e2e
-    if pg is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        eng.render(job, host_outs=[host])
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / n_e2e)
     e2e_value = paths_per_step * ws / e2e_s * 1e-6
     h2d = ctypes.sizeof(sb.SnogCamera) + ctypes.sizeof(sb.SnogRenderParams)
     d2h = WIDTH * HEIGHT * 3 * 4
+    eng.close()
 
     # ---- CPU baseline (rank 0, N=1) and algorithmic bytes ------------------
     cpu = None
@@ -322,7 +487,6 @@ def bench_ours(args):
                        "kind": "reference",
                        "sample": f"{WIDTH}x{HEIGHT} at 2 spp (of {SPP}), all rows, "
                                  f"{r['seconds']:.1f} s"}
-    roofline = None
     peaks = {}
     pk_path = os.path.join(HERE, "MEASURED_PEAKS.json")
     if os.path.exists(pk_path):
@@ -330,24 +494,36 @@ def bench_ours(args):
             peaks = json.load(f)
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    if prof["closest_launches"]:
-        per_launch_ms = prof["closest_ms"] / prof["closest_launches"]
-        rays_per_launch = prof["closest_rays"] / prof["closest_launches"]
+    roofline = None
+    if prof["iterations"] and prof["closest_ms"] > 0:
+        per_launch_ms = prof["closest_ms"] / prof["iterations"]
+        rays_per_launch = prof["closest_rays"] / prof["iterations"]
         if bytes_ray is not None:
-            b_ray, src = bytes_ray[0], "reference traversal counts"
+            b_ray, src = bytes_ray[0], "reference traversal counts (RenderStats::IsecStats)"
         else:
-            # own counts: nodes entered and primitives tested by the kernel
-            b_ray = 36 + (36 * prof["closest_nodes"] + 40 * prof["closest_tests"]) / max(
-                prof["closest_rays"], 1)
-            src = "kernel's own traversal counts"
-        achieved = b_ray * rays_per_launch / (per_launch_ms * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "kernel": "k_trace_closest", "achieved": round(achieved, 1),
-                    "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                    "peak_source": peak_src, "bytes_per_ray": round(b_ray, 1),
-                    "bytes_source": src, "rays_per_launch": round(rays_per_launch),
-                    "ms_per_launch": round(per_launch_ms, 4), "traffic": None,
-                    "kernel_share": {k: round(prof[k + "_ms"] / max(prof["device_ms"], 1e-9), 4)
+            b_ray, src = None, "unavailable"
+        traffic_ray = read_traffic_per_ray()
+        device_ms = prof["closest_ms"] + prof["shadow_ms"] + prof["shade_ms"] + prof["other_ms"]
+        roofline = {"bound": "hbm", "kernel": "k_e_closest", "peak": peak, "unit": "GB/s",
+                    "peak_source": peak_src, "bytes_source": src,
+                    "rays_per_launch": round(rays_per_launch), "ms_per_launch": round(per_launch_ms, 4),
+                    "kernel_share": {k: round(prof[k + "_ms"] / max(device_ms, 1e-9), 4)
                                      for k in ("closest", "shadow", "shade", "other")}}
+        if b_ray is not None:
+            achieved = b_ray * rays_per_launch / (per_launch_ms * 1e-3) / 1e9
+            roofline.update({"achieved": round(achieved, 1), "frac": round(achieved / peak, 4),
+                             "bytes_per_ray": round(b_ray, 1)})
+        else:
+            roofline.update({"achieved": None, "frac": None})
+        roofline["traffic"] = round(traffic_ray * rays_per_launch) if traffic_ray else None
+        roofline["traffic_per_ray"] = traffic_ray
+
+    batched = serve = None
+    if rank == 0 and ws == 1:
+        if args.batch_jobs:
+            batched = bench_batch(args, sb, scenes, torch, stream)
+        if args.serve_requests:
+            serve = bench_serve(args, sb, scenes)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 4), "unit": "Mpaths/s", "n_gpus": ws,
@@ -356,15 +532,18 @@ def bench_ours(args):
                 "data": "synthetic (seeded terrain scene; inputs larger than L2, no flush)",
                 "config": {"workload": "terrain-2M-tris+200-spheres+sky-envmap", "width": WIDTH,
                            "height": HEIGHT, "spp": SPP, "max_path_len": MAX_LEN,
-                           "parallelism": f"replicas x{ws}", "l2": "working set > L2"},
-                "gpu_launches": launches * args.steps,
+                           "parallelism": f"replicas x{ws}", "l2": "working set > L2",
+                           "engine": _cfg_dict(cfg)},
+                "gpu_launches": launches,
                 "e2e": {"value": round(e2e_value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
+                "plain": {"value": round(paths_per_step * ws / plain_ms * 1e-3, 4), "unit": "Mpaths/s",
+                          "ms_per_step": round(plain_ms, 3)},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-                "rays": {"closest_per_step": prof["closest_rays"],
-                         "shadow_per_step": prof["shadow_rays"],
-                         "mrays_per_s": round((prof["closest_rays"] + prof["shadow_rays"]) * ws
-                                              / ms * 1e-3, 2)}}
+                "rays": {"closest_per_step": rays[0] // max(args.steps, 1),
+                         "shadow_per_step": rays[1] // max(args.steps, 1),
+                         "mrays_per_s": round((rays[0] + rays[1]) * ws / (ms * args.steps) * 1e-3, 2)},
+                "batched": batched, "serve": serve}
         print(json.dumps(line))
     scene.close()
     if pg is not None:
@@ -386,7 +565,14 @@ def main():
     ap.add_argument("--isec-only", action="store_true",
                     help="only the intersection-only batch (1M triangles, 16M rays)")
     ap.add_argument("--isec-rays", type=int, default=0)
+    ap.add_argument("--batch-jobs", type=int, default=1024,
+                    help="jobs of the batched workload (0 = skip it)")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="requests of the serving workload per rate (0 = skip it; 2000 = full stream)")
+    ap.add_argument("--serve-rates", type=str, default="100",
+                    help="comma-separated Poisson arrival rates, requests/s")
     args = ap.parse_args()
+    args.serve_rates = [float(x) for x in args.serve_rates.split(",") if x]
     WIDTH, HEIGHT, SPP = args.width, args.height, args.spp
     if args.warmup < 3:
         args.warmup = 3

@@ -223,6 +223,8 @@ typedef struct SnogEngineConfig {
   uint32_t max_jobs;          /* jobs admitted at once */
   uint32_t max_lights;        /* light samples per vertex (lights x direct_samples) */
   uint32_t iters_per_launch;  /* iteration pairs per graph launch */
+  uint32_t max_scenes;        /* scene table entries */
+  uint32_t reserved;          /* 0 */
   uint64_t mem_budget;        /* device bytes for per-job buffers (admission) */
 } SnogEngineConfig;
 
@@ -236,11 +238,33 @@ typedef struct SnogBatchStats {
   uint64_t paths, closest_rays, shadow_rays;
   double wall_ms;
   uint32_t kernel_launches;
+  uint32_t iterations;        /* the rest only with SNOG_PROFILE_KERNELS=1 */
+  double closest_ms, shadow_ms, shade_ms, other_ms;   /* device time per kernel kind */
 } SnogBatchStats;
 
 /* Defaults: 16M slots, 64K-path items, 16K-item ring, 4096 jobs, 4 light
- * samples, 4 iteration pairs per launch, 120 GB budget. */
+ * samples, 4 iteration pairs per launch, 1024 scenes, 120 GB budget. */
 int snog_engine_default_config(SnogEngineConfig *cfg);
+
+/* A persistent engine: its queues (the bulk of its memory) and CUDA graph
+ * stay allocated between renders.  STREAM is the caller's cudaStream_t or
+ * NULL for a stream of its own; all its work is ordered on that stream. */
+typedef struct SnogEngine SnogEngine;
+int snog_engine_create(const SnogEngineConfig *cfg, void *stream, SnogEngine **out);
+/* Render N_JOBS jobs to completion (as snog_render_batch). */
+int snog_engine_render(SnogEngine *engine, SnogScene *const *scenes, const SnogCamera *cameras,
+                       const SnogRenderParams *params, uint32_t n_jobs, float *const *outs, int outs_on_device,
+                       SnogBatchStats *stats);
+int snog_engine_destroy(SnogEngine *engine);
+
+/* Pick slots (queue depth), item_paths (scheduling grain) and
+ * iters_per_launch for a batch by timing candidates on a sample of it (each
+ * job at 1 spp, at most SAMPLE_JOBS jobs evenly spaced, 0 = 64); the rest of
+ * BASE is kept.  best_mpaths (may be NULL) receives the winner's rate on the
+ * sample. */
+int snog_engine_autotune(SnogScene *const *scenes, const SnogCamera *cameras, const SnogRenderParams *params,
+                         uint32_t n_jobs, uint32_t sample_jobs, const SnogEngineConfig *base,
+                         SnogEngineConfig *best, double *best_mpaths);
 
 /* Render N_JOBS jobs together to completion.  outs[i] receives job i's image
  * (height x width RGB floats, top row first) in host memory, or device memory

@@ -91,7 +91,7 @@ class SnogRenderStats(C.Structure):
 class SnogEngineConfig(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("item_paths", C.c_uint32), ("ring_items", C.c_uint32),
                 ("max_jobs", C.c_uint32), ("max_lights", C.c_uint32), ("iters_per_launch", C.c_uint32),
-                ("mem_budget", C.c_uint64)]
+                ("max_scenes", C.c_uint32), ("reserved", C.c_uint32), ("mem_budget", C.c_uint64)]
 
 
 class SnogJobStats(C.Structure):
@@ -101,7 +101,9 @@ class SnogJobStats(C.Structure):
 
 class SnogBatchStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("wall_ms", C.c_double), ("kernel_launches", C.c_uint32)]
+                ("wall_ms", C.c_double), ("kernel_launches", C.c_uint32), ("iterations", C.c_uint32),
+                ("closest_ms", C.c_double), ("shadow_ms", C.c_double), ("shade_ms", C.c_double),
+                ("other_ms", C.c_double)]
 
 
 def _sig(name, res, *args):
@@ -137,6 +139,15 @@ _engine_default = _sig("snog_engine_default_config", C.c_int, C.POINTER(SnogEngi
 _render_batch = _sig("snog_render_batch", C.c_int, C.POINTER(_P), C.POINTER(SnogCamera),
                      C.POINTER(SnogRenderParams), C.c_uint32, C.POINTER(_P), C.c_int,
                      C.POINTER(SnogEngineConfig), C.POINTER(SnogBatchStats))
+_engine_create = _sig("snog_engine_create", C.c_int, C.POINTER(SnogEngineConfig), _P, C.POINTER(_P))
+_engine_render = _sig("snog_engine_render", C.c_int, _P, C.POINTER(_P), C.POINTER(SnogCamera),
+                      C.POINTER(SnogRenderParams), C.c_uint32, C.POINTER(_P), C.c_int,
+                      C.POINTER(SnogBatchStats))
+_engine_destroy = _sig("snog_engine_destroy", C.c_int, _P)
+_engine_autotune = _sig("snog_engine_autotune", C.c_int, C.POINTER(_P), C.POINTER(SnogCamera),
+                        C.POINTER(SnogRenderParams), C.c_uint32, C.c_uint32,
+                        C.POINTER(SnogEngineConfig), C.POINTER(SnogEngineConfig),
+                        C.POINTER(C.c_double))
 _server_create = _sig("snog_server_create", C.c_int, C.POINTER(SnogEngineConfig), C.POINTER(_P))
 _server_add_scene = _sig("snog_server_add_scene", C.c_int, _P, _P, C.POINTER(C.c_uint32))
 _server_submit = _sig("snog_server_submit", C.c_int, _P, C.c_uint32, C.POINTER(SnogCamera),
@@ -299,19 +310,84 @@ def engine_config(**kw):
     return c
 
 
-def render_batch(jobs, config=None):
-    """Render [(Scene, Camera, RenderParams), ...] together on the streaming
-    engine.  Returns (list of (H, W, 3) float32 images, stats dict)."""
+def _job_arrays(jobs):
     n = len(jobs)
     scenes = (_P * n)(*[j[0].handle for j in jobs])
     cams = (SnogCamera * n)(*[camera_struct(j[1]) for j in jobs])
     prms = (SnogRenderParams * n)(*[params_struct(j[2]) for j in jobs])
-    outs = [np.empty((j[2].height, j[2].width, 3), np.float32) for j in jobs]
-    optr = (_P * n)(*[o.ctypes.data for o in outs])
+    return n, scenes, cams, prms
+
+
+def _out_arrays(jobs, outs):
+    if outs is None:
+        outs = [np.empty((j[2].height, j[2].width, 3), np.float32) for j in jobs]
+        ptrs = [o.ctypes.data for o in outs]
+    else:   # device pointers (ints) or arrays
+        ptrs = [o if isinstance(o, int) else o.ctypes.data for o in outs]
+    return outs, (_P * len(jobs))(*ptrs)
+
+
+def _batch_stats(st):
+    return {f: getattr(st, f) for f, _ in SnogBatchStats._fields_}
+
+
+def render_batch(jobs, config=None):
+    """Render [(Scene, Camera, RenderParams), ...] together on the streaming
+    engine.  Returns (list of (H, W, 3) float32 images, stats dict)."""
+    n, scenes, cams, prms = _job_arrays(jobs)
+    outs, optr = _out_arrays(jobs, None)
     st = SnogBatchStats()
     _check(_render_batch(scenes, cams, prms, n, optr, 0, C.byref(config) if config else None,
                          C.byref(st)))
-    return outs, {f: getattr(st, f) for f, _ in SnogBatchStats._fields_}
+    return outs, _batch_stats(st)
+
+
+def autotune(jobs, sample_jobs=0, base=None):
+    """Engine configuration tuned on a sample of JOBS; returns (config, Mpaths/s on the sample)."""
+    n, scenes, cams, prms = _job_arrays(jobs)
+    best = SnogEngineConfig()
+    rate = C.c_double()
+    _check(_engine_autotune(scenes, cams, prms, n, sample_jobs, C.byref(base) if base else None,
+                            C.byref(best), C.byref(rate)))
+    return best, rate.value
+
+
+class Engine:
+    """A persistent streaming engine (snog_engine_*): queues and CUDA graph
+    stay allocated between batches.  STREAM: a cudaStream_t as int, or 0."""
+
+    def __init__(self, config=None, stream=0):
+        h = _P()
+        _check(_engine_create(C.byref(config) if config else None, stream or None, C.byref(h)))
+        self._h = h
+
+    def render(self, jobs, device_outs=None, host_outs=None):
+        """Render JOBS to completion.  Images go to DEVICE_OUTS (device
+        pointers, one per job), else to HOST_OUTS ((H, W, 3) float32 arrays,
+        e.g. pinned), else to new host arrays, which are returned."""
+        n, scenes, cams, prms = _job_arrays(jobs)
+        outs, optr = _out_arrays(jobs, device_outs if device_outs else host_outs)
+        st = SnogBatchStats()
+        _check(_engine_render(self._h, scenes, cams, prms, n, optr, 1 if device_outs else 0,
+                              C.byref(st)))
+        return (None if device_outs else outs), _batch_stats(st)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(_engine_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

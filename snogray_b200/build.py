@@ -24,7 +24,10 @@ NVCC = shutil.which("nvcc") or os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
             "-Wno-unused-function", f"-I{CUDA}/include", f"-I{INCLUDE}"]
-NVCCFLAGS = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC",
+# -fmad=false: every float operation rounds on its own, as in the reference's
+# parity build (-ffp-contract=off), so the same shading code compiled into two
+# kernels (the wave renderer and the streaming engine) gives the same bits.
+NVCCFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", *ARCH, "-Xcompiler", "-fPIC",
              "--expt-relaxed-constexpr", f"-I{INCLUDE}", "-Xptxas", "-warn-spills"]
 
 

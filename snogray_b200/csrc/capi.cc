@@ -5,8 +5,10 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <new>
 #include <string>
@@ -83,8 +85,6 @@ struct DevBuf {
 
 void RenderCache::release() {
   wave_free(wb);
-  cudaFree(trace_scratch);
-  trace_scratch = nullptr;
   cudaFree(accum);
   cudaFree(wsum);
   cudaFree(out);
@@ -94,10 +94,10 @@ void RenderCache::release() {
   npix_cap = 0;
 }
 
-// Paths per wave: SNOG_WAVE_PATHS if set, else 4M, limited to what fits in
+// Paths per wave: SNOG_WAVE_PATHS if set, else 16M, limited to what fits in
 // a quarter of the free device memory and to the job's own path count.
 static uint64_t choose_wave_cap(uint64_t total_paths, uint32_t spp, uint32_t n_lights) {
-  uint64_t cap = 1ull << 22;
+  uint64_t cap = 1ull << 24;
   if (const char *e = getenv("SNOG_WAVE_PATHS")) cap = strtoull(e, nullptr, 10);
   size_t free_b = 0, tot_b = 0;
   if (cudaMemGetInfo(&free_b, &tot_b) == cudaSuccess) {
@@ -115,30 +115,49 @@ static void check_params(const SnogRenderParams &p) {
     throw Error{SNOG_EINVAL, "width, height and spp must be positive"};
   if (p.width > 65536 || p.height > 65536) throw Error{SNOG_EINVAL, "image too large"};
   if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};
+  if (p.direct_samples > 64) throw Error{SNOG_EINVAL, "direct_samples must be <= 64"};
   if (uint64_t(p.width + 4) * (p.height + 4) * p.spp >= (1ull << 40))
     throw Error{SNOG_EINVAL, "too many paths in one job"};
   if (uint64_t(p.width + 4) * (p.height + 4) >= (1ull << 32))
     throw Error{SNOG_EINVAL, "render pattern too large"};
 }
 
-// Render into the scene's cached accumulator; the resolved image goes to
-// d_out (device).  Caller holds the scene lock.
+RenderPool &render_pool(int device) {
+  static std::mutex mu;
+  static std::map<int, std::unique_ptr<RenderPool>> pools;
+  std::lock_guard<std::mutex> lk(mu);
+  auto &p = pools[device];
+  if (!p) p.reset(new RenderPool);
+  return *p;
+}
+
+// Render with the device's pooled working memory; the resolved image goes to
+// d_out (device) or, if null, to h_out (host, copied before returning).
 static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
-                        cudaStream_t st, SnogRenderStats *stats) {
+                        float *h_out, cudaStream_t st, SnogRenderStats *stats) {
   check_params(p);
   if (!stack_class_for_depth(S.dev.max_depth))
     throw Error{SNOG_EINVAL, "octree deeper than the traversal kernels support (84 levels)"};
-  RenderCache &rc = S.rc;
+  RenderPool &pool = render_pool(S.device);
+  std::lock_guard<std::mutex> plk(pool.mu);
+  if (!pool.done) check_cuda(cudaEventCreateWithFlags(&pool.done, cudaEventDisableTiming), "event");
+  RenderCache &rc = pool.rc;
   const uint64_t total = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
-  uint64_t cap = choose_wave_cap(total, p.spp, S.dev.n_lights);
-  if (rc.wb.wave_cap < cap || rc.wb.n_lights != S.dev.n_lights) {
-    cudaError_t e = wave_alloc(rc.wb, cap, S.dev.n_lights);
+  // Shadow-queue entries a vertex may need: two per light sample.
+  const uint32_t ls = std::max(1u, S.dev.n_lights) * std::max(1u, p.direct_samples);
+  uint64_t cap = choose_wave_cap(total, p.spp, ls);
+  const size_t npix = size_t(p.width) * p.height;
+  const bool grow = rc.wb.wave_cap < cap || rc.wb.n_lights < ls || rc.npix_cap < npix;
+  // Buffers about to be replaced may still be in use by a render on another stream.
+  if (grow) check_cuda(cudaEventSynchronize(pool.done), "pool wait");
+  check_cuda(cudaStreamWaitEvent(st, pool.done, 0), "pool order");
+  if (rc.wb.wave_cap < cap || rc.wb.n_lights < ls) {
+    cudaError_t e = wave_alloc(rc.wb, std::max<uint64_t>(cap, rc.wb.wave_cap), std::max(ls, rc.wb.n_lights));
     if (e != cudaSuccess) {
       cudaGetLastError();
       throw Error{SNOG_ENOMEM, std::string("wave buffers: ") + cudaGetErrorString(e)};
     }
   }
-  const size_t npix = size_t(p.width) * p.height;
   if (rc.npix_cap < npix) {
     cudaFree(rc.accum);
     cudaFree(rc.wsum);
@@ -163,8 +182,14 @@ static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderPar
   const char *pe = getenv("SNOG_PROFILE_KERNELS");
   const bool profile = stats && pe && pe[0] == '1';
   RenderProfile prof;
-  cudaError_t e = render_job(S.dev, jc, rc.wb, rc.accum, rc.wsum, d_out ? d_out : rc.out, st, &waves,
+  WaveBuffers wave = rc.wb;   // the pool may be larger than this job's wave
+  wave.wave_cap = cap;
+  cudaError_t e = render_job(S.dev, jc, wave, rc.accum, rc.wsum, d_out ? d_out : rc.out, st, &waves,
                              &launches, profile ? &prof : nullptr);
+  if (e == cudaSuccess && !d_out)
+    e = cudaMemcpyAsync(h_out, rc.out, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaEventRecord(pool.done, st);
+  if (e == cudaSuccess && !d_out) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -217,11 +242,7 @@ int snog_render(SnogScene *scene, const SnogCamera *camera, const SnogRenderPara
     SceneImpl &S = *scene->impl;
     if (!S.on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
     std::lock_guard<std::mutex> lk(S.mu);
-    SnogRenderStats local{};
-    render_into(S, *camera, *params, nullptr, nullptr, stats ? stats : &local);
-    check_cuda(cudaMemcpy(out_rgb, S.rc.out, size_t(params->width) * params->height * 3 * sizeof(float),
-                          cudaMemcpyDeviceToHost),
-               "image D2H");
+    render_into(S, *camera, *params, nullptr, out_rgb, nullptr, stats);
     return int(SNOG_OK);
   });
 }
@@ -233,7 +254,7 @@ int snog_render_device(SnogScene *scene, const SnogCamera *camera, const SnogRen
     SceneImpl &S = *scene->impl;
     if (!S.on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
     std::lock_guard<std::mutex> lk(S.mu);
-    render_into(S, *camera, *params, d_out_rgb, cudaStream_t(stream), stats);
+    render_into(S, *camera, *params, d_out_rgb, nullptr, cudaStream_t(stream), stats);
     return int(SNOG_OK);
   });
 }
@@ -275,7 +296,7 @@ int snog_scene_destroy(SnogScene *scene) {
     if (!scene) return int(SNOG_OK);
     {
       std::lock_guard<std::mutex> lk(scene->impl->mu);
-      scene->impl->rc.release();
+      cudaFree(scene->impl->trace_scratch);
       scene->impl->arena.release();
     }
     delete scene->impl;
@@ -319,10 +340,10 @@ int snog_trace_device(SnogScene *scene, const float *d_rays, uint32_t n, uint32_
     if (!stack_class_for_depth(S.dev.max_depth))
       throw Error{SNOG_EINVAL, "octree deeper than the traversal kernels support (84 levels)"};
     std::lock_guard<std::mutex> lk(S.mu);
-    if (!S.rc.trace_scratch) check_cuda(cudaMalloc(&S.rc.trace_scratch, 64), "trace scratch");
-    check_cuda(cudaMemsetAsync(S.rc.trace_scratch, 0, 64, cudaStream_t(stream)), "memset");
+    if (!S.trace_scratch) check_cuda(cudaMalloc(&S.trace_scratch, 64), "trace scratch");
+    check_cuda(cudaMemsetAsync(S.trace_scratch, 0, 64, cudaStream_t(stream)), "memset");
     check_cuda(launch_trace_batch(S.dev, d_rays, n, n_closest, d_prim, d_t, d_normal, nullptr,
-                                  S.rc.trace_scratch + 1, S.rc.trace_scratch, cudaStream_t(stream), nullptr),
+                                  S.trace_scratch + 1, S.trace_scratch, cudaStream_t(stream), nullptr),
                "trace launch");
     return int(SNOG_OK);
   });

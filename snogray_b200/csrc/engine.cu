@@ -86,7 +86,8 @@ __global__ void __launch_bounds__(256) k_e_regen(EngineCtl *ctl, const WorkItem 
                          mul(mul(load3(jc.cam_up), y), jc.tan_y));
     const uint32_t slot = base + t;
     q.o[slot] = make_float4(jc.cam_pos[0], jc.cam_pos[1], jc.cam_pos[2], 0.f);
-    q.d[slot] = make_float4(d.x, d.y, d.z, jc.max_trace);
+    // A cancelled job's new paths get an empty ray interval (nothing to trace).
+    q.d[slot] = make_float4(d.x, d.y, d.z, J.canceled ? 0.f : jc.max_trace);
     q.thr[slot] = make_float4(1.f, 1.f, 1.f, 1.f);
     q.rad[slot] = make_float4(0.f, 0.f, 0.f, 1.f);
     q.meta[slot] = make_uint4(0u, job, uint32_t(g), uint32_t(g >> 32));
@@ -194,6 +195,9 @@ __global__ void __launch_bounds__(128) k_e_shade(EngineCtl *ctl, uint32_t cur, c
       J = jobs + job;
       scene = J->scene;
       s = scenes + scene;
+    }
+    const bool retire = active && J->canceled;   // cancelled job: the path ends here, unshaded
+    if (active && !retire) {
       o4 = qin.o[i];
       d4 = qin.d[i];
       ref = hit_ref[i];
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(128) k_e_shade(EngineCtl *ctl, uint32_t cur, c
     }
     const uint32_t slot = warp_append(count_out, cont);
     float4 *target = nullptr;
-    if (active) {
+    if (active && !retire) {
       if (cont) {
         const JobConsts &jc = J->jc;
         qout.o[slot] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
@@ -374,27 +378,88 @@ __global__ void __launch_bounds__(128) k_e_shade(EngineCtl *ctl, uint32_t cur, c
   }
 }
 
+// One iteration's kernel sequence on ST.  EV (null while capturing a graph)
+// receives five events: before plan, before closest, before shade, before
+// shadow, after shadow.
 template <int STACK>
-void capture_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N,
-                       uint32_t cur, const EngineJobDev *jobs, const DevScene *scenes, EQ qc, EQ qn,
-                       uint32_t *hit_ref, float *hit_t, ESQ sq, unsigned long long *job_done) {
+void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N,
+                      uint32_t cur, const EngineJobDev *jobs, const DevScene *scenes, EQ qc, EQ qn,
+                      uint32_t *hit_ref, float *hit_t, ESQ sq, unsigned long long *job_done,
+                      const cudaEvent_t *ev) {
   const uint32_t sms = uint32_t(num_sms());
+  if (ev) cudaEventRecord(ev[0], st);
   k_e_plan<<<1, 1, 0, st>>>(ctl, ring, R, N, cur);
   k_e_regen<<<sms * 8, 256, 0, st>>>(ctl, ring, R, jobs, qc);
+  if (ev) cudaEventRecord(ev[1], st);
   k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, 128), 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
                                                                                hit_t);
+  if (ev) cudaEventRecord(ev[2], st);
   k_e_shade<<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done);
+  if (ev) cudaEventRecord(ev[3], st);
   k_e_shadow<STACK><<<resident_grid(k_e_shadow<STACK>, 128), 128, 0, st>>>(ctl, scenes, sq);
+  if (ev) cudaEventRecord(ev[4], st);
 }
 
 }  // namespace
 
-Engine::Engine(const EngineConfigHost &cfg) : cfg_(cfg) {
+size_t BlockCache::round_up(size_t n) {
+  if (n <= 4096) return 4096;
+  size_t p = 1;
+  while (p <= n / 2) p <<= 1;     // largest power of two <= n
+  const size_t step = p / 8;
+  return (n + step - 1) / step * step;
+}
+
+void *BlockCache::get(size_t n) {
+  const size_t r = round_up(n);
+  auto it = free_.lower_bound(r);
+  if (it != free_.end() && it->first <= r + r / 4) {
+    void *p = it->second;
+    free_.erase(it);
+    return p;
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, r) != cudaSuccess) {
+    cudaGetLastError();
+    trim();
+    if (cudaMalloc(&p, r) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+  }
+  size_of_[p] = r;
+  held_ += r;
+  return p;
+}
+
+void BlockCache::put(void *p) {
+  if (!p) return;
+  auto it = size_of_.find(p);
+  if (it != size_of_.end()) free_.insert({it->second, p});
+}
+
+void BlockCache::trim() {
+  for (auto &kv : free_) {
+    cudaFree(kv.second);
+    held_ -= size_of_[kv.second];
+    size_of_.erase(kv.second);
+  }
+  free_.clear();
+}
+
+Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
   t0_ = std::chrono::steady_clock::now();
-  if (cfg_.slots < 1024 || cfg_.item_paths == 0 || cfg_.ring_items < 16 || cfg_.max_jobs == 0 ||
-      cfg_.iters_per_launch == 0)
+  if (cfg_.slots < 1024 || cfg_.slots > (1u << 30) || cfg_.item_paths == 0 || cfg_.ring_items < 16 ||
+      cfg_.max_jobs == 0 || cfg_.iters_per_launch == 0 || cfg_.iters_per_launch > 64 || cfg_.max_scenes == 0 ||
+      cfg_.max_lights > 256)
     throw Error{SNOG_EINVAL, "engine config out of range"};
-  check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  max_scenes_ = cfg_.max_scenes;
+  if (stream) {
+    stream_ = stream;
+  } else {
+    check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    own_stream_ = true;
+  }
   const size_t N = cfg_.slots, L = cfg_.max_lights ? cfg_.max_lights : 1;
   size_t off = 0;
   auto take = [&](size_t b) {
@@ -435,6 +500,8 @@ Engine::Engine(const EngineConfigHost &cfg) : cfg_(cfg) {
   check_cuda(cudaMemsetAsync(job_done_, 0, 8 * size_t(cfg_.max_jobs), stream_), "memset");
   check_cuda(cudaMallocHost(&ctl_host_, sizeof(EngineCtl)), "pinned");
   check_cuda(cudaMallocHost(&done_host_, 8 * size_t(cfg_.max_jobs)), "pinned");
+  staging_cap_ = size_t(cfg_.max_jobs) * sizeof(EngineJobDev) + size_t(cfg_.ring_items) * sizeof(WorkItem) + 4096;
+  check_cuda(cudaMallocHost(&staging_, staging_cap_), "pinned staging");
   std::memset(done_host_, 0, 8 * size_t(cfg_.max_jobs));
   for (uint32_t k = cfg_.max_jobs; k > 0; k--) free_slots_.push_back(k - 1);
   check_cuda(cudaStreamSynchronize(stream_), "engine init");
@@ -444,10 +511,25 @@ Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto &kv : jobs_) release_job(kv.second);
   if (graph_) cudaGraphExecDestroy(graph_);
+  cache_.trim();
   cudaFree(block_);
   cudaFreeHost(ctl_host_);
   cudaFreeHost(done_host_);
-  if (stream_) cudaStreamDestroy(stream_);
+  cudaFreeHost(staging_);
+  for (cudaEvent_t e : events_) cudaEventDestroy(e);
+  if (own_stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::reset_scenes() {
+  if (!jobs_.empty()) throw Error{SNOG_EBUSY, "engine has jobs in flight"};
+  scenes_.clear();
+}
+
+void Engine::clear_counters() {
+  prof_ = Profile{};
+  kernel_launches_ = 0;
+  base_closest_ = last_ctl_.rays_closest;
+  base_shadow_ = last_ctl_.rays_shadow;
 }
 
 double Engine::now_ms() const {
@@ -475,22 +557,43 @@ uint32_t Engine::add_scene(SceneImpl *scene) {
   return slot;
 }
 
-void Engine::build_graph() {
+// Every iteration of one launch (iters_per_launch pairs, queue 0 -> 1 -> 0),
+// with events around the kernels while profiling.
+void Engine::launch_iterations() {
   EQ q[2];
   for (int k = 0; k < 2; k++) q[k] = EQ{q_o_[k], q_d_[k], q_thr_[k], q_rad_[k], q_meta_[k]};
   ESQ sq{s_o_, s_d_, s_c_, s_tgt_};
-  cudaGraph_t g;
-  check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
-  for (uint32_t it = 0; it < cfg_.iters_per_launch; it++) {
-    for (uint32_t cur = 0; cur < 2; cur++) {
-      switch (graph_stack_) {
-        case 32: capture_iteration<32>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
-        case 64: capture_iteration<64>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
-        case 128: capture_iteration<128>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
-        default: capture_iteration<256>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_); break;
-      }
+  const uint32_t n_iter = 2 * cfg_.iters_per_launch;
+  if (profile_on_ && events_.size() < 5 * size_t(n_iter)) {
+    while (events_.size() < 5 * size_t(n_iter)) {
+      cudaEvent_t e;
+      check_cuda(cudaEventCreate(&e), "event");
+      events_.push_back(e);
     }
   }
+  for (uint32_t it = 0; it < n_iter; it++) {
+    const uint32_t cur = it & 1u;
+    const cudaEvent_t *ev = profile_on_ ? &events_[5 * it] : nullptr;
+#define SNOG_ITER(S)                                                                                          \
+  launch_iteration<S>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], \
+                      q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_, ev)
+    switch (graph_stack_) {
+      case 32: SNOG_ITER(32); break;
+      case 64: SNOG_ITER(64); break;
+      case 128: SNOG_ITER(128); break;
+      default: SNOG_ITER(256); break;
+    }
+#undef SNOG_ITER
+  }
+}
+
+void Engine::build_graph() {
+  cudaGraph_t g;
+  const bool prof = profile_on_;
+  profile_on_ = false;
+  check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+  launch_iterations();
+  profile_on_ = prof;
   cudaError_t e = cudaStreamEndCapture(stream_, &g);
   check_cuda(e, "end capture");
   e = cudaGraphInstantiate(&graph_, g, 0);
@@ -534,16 +637,29 @@ bool Engine::cancel(uint64_t id) {
 }
 
 void Engine::release_job(HostJob &j) {
-  cudaFree(j.result);
-  cudaFree(j.jit);
-  cudaFree(j.accum);
-  cudaFree(j.wsum);
-  if (!j.out_on_device) cudaFree(j.dev_out);
+  cache_.put(j.result);
+  cache_.put(j.jit);
+  cache_.put(j.accum);
+  cache_.put(j.wsum);
+  if (!j.out_on_device) cache_.put(j.dev_out);
   j.result = nullptr;
   j.jit = nullptr;
   j.accum = nullptr;
   j.wsum = nullptr;
   j.dev_out = nullptr;
+}
+
+void *Engine::stage(const void *src, size_t n) {
+  const size_t need = (n + 15) & ~size_t(15);
+  if (staging_used_ + need > staging_cap_) {
+    // Everything staged so far must have been copied before the area is reused.
+    check_cuda(cudaStreamSynchronize(stream_), "staging");
+    staging_used_ = 0;
+  }
+  char *p = staging_ + staging_used_;
+  std::memcpy(p, src, n);
+  staging_used_ += need;
+  return p;
 }
 
 // Admit pending jobs in arrival order while the memory budget and the job
@@ -560,12 +676,8 @@ void Engine::admit() {
     }
     if (free_slots_.empty() || budget_used_ + j.bytes > cfg_.mem_budget) break;
     auto alloc = [&](void **p, size_t n) {
-      cudaError_t e = cudaMalloc(p, n);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-      }
-      return true;
+      *p = cache_.get(n);
+      return *p != nullptr;
     };
     bool ok = alloc(reinterpret_cast<void **>(&j.result), j.total * 16) &&
               alloc(reinterpret_cast<void **>(&j.jit), j.total * 8) &&
@@ -594,7 +706,8 @@ void Engine::admit() {
     rec.total = j.total;
     rec.result = j.result;
     rec.jit = j.jit;
-    check_cuda(cudaMemcpyAsync(jobs_dev_ + j.table_slot, &rec, sizeof rec, cudaMemcpyHostToDevice, stream_),
+    check_cuda(cudaMemcpyAsync(jobs_dev_ + j.table_slot, stage(&rec, sizeof rec), sizeof rec,
+                               cudaMemcpyHostToDevice, stream_),
                "job record");
     check_cuda(cudaMemsetAsync(job_done_ + j.table_slot, 0, 8, stream_), "job counter");
     done_host_[j.table_slot] = 0;
@@ -636,8 +749,8 @@ void Engine::push_items() {
   while (k < batch.size()) {
     const uint64_t slot = pos % R;
     const size_t run = std::min<size_t>(batch.size() - k, size_t(R - slot));
-    check_cuda(cudaMemcpyAsync(ring_ + slot, batch.data() + k, run * sizeof(WorkItem), cudaMemcpyHostToDevice,
-                               stream_),
+    check_cuda(cudaMemcpyAsync(ring_ + slot, stage(batch.data() + k, run * sizeof(WorkItem)),
+                               run * sizeof(WorkItem), cudaMemcpyHostToDevice, stream_),
                "ring push");
     k += run;
     pos += run;
@@ -645,55 +758,90 @@ void Engine::push_items() {
   pushed_tail_ = pos;
   // tail and avail_end are adjacent fields of the control block
   unsigned long long pub[2] = {pushed_tail_, pushed_cum_};
-  check_cuda(cudaMemcpyAsync(&ctl_->item_tail, pub, sizeof pub, cudaMemcpyHostToDevice, stream_), "ring tail");
-  check_cuda(cudaStreamSynchronize(stream_), "ring push");   // pub is on the stack
-}
-
-void Engine::finish_job(HostJob &j) {
-  cudaError_t e = splat_job(j.jc, j.result, j.jit, j.total, j.accum, j.wsum, j.dev_out, stream_);
-  check_cuda(e, "splat");
-  kernel_launches_ += 2;
-  if (!j.out_on_device)
-    check_cuda(cudaMemcpyAsync(j.out, j.dev_out, j.npix * 12, cudaMemcpyDeviceToHost, stream_), "image D2H");
-  check_cuda(cudaStreamSynchronize(stream_), "finish");
-  j.st.finish_ms = now_ms();
-  j.st.status = SNOG_OK;
+  check_cuda(cudaMemcpyAsync(&ctl_->item_tail, stage(pub, sizeof pub), sizeof pub, cudaMemcpyHostToDevice, stream_),
+             "ring tail");
 }
 
 bool Engine::step() {
+  if (staging_used_) {
+    check_cuda(cudaStreamSynchronize(stream_), "staging");   // earlier staged copies done
+    staging_used_ = 0;
+  }
   admit();
+  // Tell the device about cancellations: the job's queued paths retire.
+  for (uint64_t id : active_) {
+    HostJob &j = jobs_.at(id);
+    if (j.canceled && !j.cancel_sent) {
+      const uint32_t one = 1;
+      check_cuda(cudaMemcpyAsync(&jobs_dev_[j.table_slot].canceled, stage(&one, sizeof one), sizeof one,
+                                 cudaMemcpyHostToDevice, stream_),
+                 "cancel flag");
+      j.cancel_sent = true;
+    }
+  }
   push_items();
   // After a launch (an even number of iterations) the live rays are in queue 0.
   const bool inflight = last_ctl_.qcount[0] > 0 || last_ctl_.ticket < pushed_cum_;
   if (!inflight && active_.empty() && pending_.empty()) return false;
   if (inflight || !active_.empty()) {
-    if (!graph_) build_graph();
-    check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+    if (profile_on_) {
+      launch_iterations();
+    } else {
+      if (!graph_) build_graph();
+      check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+    }
     kernel_launches_ += 5 * 2 * cfg_.iters_per_launch;
     check_cuda(cudaMemcpyAsync(ctl_host_, ctl_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_), "ctl");
     check_cuda(cudaMemcpyAsync(done_host_, job_done_, 8 * size_t(cfg_.max_jobs), cudaMemcpyDeviceToHost, stream_),
                "done");
     check_cuda(cudaStreamSynchronize(stream_), "iteration");
+    staging_used_ = 0;
     last_ctl_ = *ctl_host_;
     if (last_ctl_.err) throw Error{SNOG_EINVAL, "traversal stack overflow (non-finite ray?)"};
+    if (profile_on_) {
+      for (uint32_t it = 0; it < 2 * cfg_.iters_per_launch; it++) {
+        const cudaEvent_t *ev = &events_[5 * it];
+        float ms[4];
+        for (int k = 0; k < 4; k++) check_cuda(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]), "event time");
+        prof_.other_ms += ms[0];
+        prof_.closest_ms += ms[1];
+        prof_.shade_ms += ms[2];
+        prof_.shadow_ms += ms[3];
+      }
+      prof_.iterations += 2 * cfg_.iters_per_launch;
+    }
   }
-  // Completed (or cancelled and drained) jobs.
-  for (size_t k = 0; k < active_.size();) {
+  // Completed (or cancelled and drained) jobs: filter every finished job's
+  // samples into its image (and copy host images back), one sync for all.
+  std::vector<size_t> done_idx;
+  bool copies = false;
+  for (size_t k = 0; k < active_.size(); k++) {
     HostJob &j = jobs_.at(active_[k]);
     const uint64_t done = done_host_[j.table_slot];
-    const bool drained = done >= j.pushed;
-    if ((done >= j.total) || (j.canceled && drained)) {
-      if (!j.canceled) finish_job(j);
-      else j.st.status = SNOG_ECANCELED, j.st.finish_ms = now_ms();
-      budget_used_ -= j.bytes;
-      release_job(j);
-      free_slots_.push_back(j.table_slot);
-      finished_[j.id] = j.st;
-      jobs_.erase(j.id);
-      active_.erase(active_.begin() + long(k));
-      continue;
+    if (done >= j.total || (j.canceled && done >= j.pushed)) {
+      done_idx.push_back(k);
+      if (done >= j.total && !j.cancel_sent) {   // complete before any cancel reached the device
+        check_cuda(splat_job(j.jc, j.result, j.jit, j.total, j.accum, j.wsum, j.dev_out, stream_), "splat");
+        kernel_launches_ += 2;
+        if (!j.out_on_device)
+          check_cuda(cudaMemcpyAsync(j.out, j.dev_out, j.npix * 12, cudaMemcpyDeviceToHost, stream_), "image D2H");
+        copies = true;
+      }
     }
-    k++;
+  }
+  if (copies) check_cuda(cudaStreamSynchronize(stream_), "finish");
+  const double t_fin = now_ms();
+  for (size_t r = done_idx.size(); r-- > 0;) {
+    const size_t k = done_idx[r];
+    HostJob &j = jobs_.at(active_[k]);
+    j.st.status = (done_host_[j.table_slot] >= j.total && !j.cancel_sent) ? SNOG_OK : SNOG_ECANCELED;
+    j.st.finish_ms = t_fin;
+    budget_used_ -= j.bytes;
+    release_job(j);
+    free_slots_.push_back(j.table_slot);
+    finished_[j.id] = j.st;
+    jobs_.erase(j.id);
+    active_.erase(active_.begin() + long(k));
   }
   return true;
 }

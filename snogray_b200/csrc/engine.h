@@ -41,7 +41,7 @@ namespace snog {
 struct EngineJobDev {
   JobConsts jc;
   uint32_t scene;          // index into the engine's scene table
-  uint32_t pad;
+  uint32_t canceled;       // set by the host: remaining paths retire unshaded
   unsigned long long total;
   float4 *result;          // per path: radiance rgb, alpha
   float2 *jit;             // per path: camera jitter in the pixel
@@ -76,6 +76,7 @@ struct EngineConfigHost {
   uint32_t max_jobs = 4096;
   uint32_t max_lights = 4;         // light samples per vertex the shadow queue holds
   uint32_t iters_per_launch = 4;
+  uint32_t max_scenes = 1024;      // scene table entries
   uint64_t mem_budget = 120ull << 30;
 };
 
@@ -85,12 +86,45 @@ struct JobStatsHost {
   int status = SNOG_EBUSY;         // SNOG_OK done, SNOG_EBUSY pending, SNOG_ECANCELED
 };
 
+// Device blocks for per-job buffers, kept for reuse instead of a cudaMalloc
+// and cudaFree per job.  Sizes are rounded up to an eighth of their power of
+// two, so a freed block serves any later request of the same class.
+class BlockCache {
+ public:
+  ~BlockCache() { trim(); }
+  void *get(size_t n);     // null if the device has no room even after trim()
+  void put(void *p);
+  void trim();             // free every cached block that is not in use
+  uint64_t held() const { return held_; }
+
+ private:
+  static size_t round_up(size_t n);
+  std::multimap<size_t, void *> free_;
+  std::map<void *, size_t> size_of_;
+  uint64_t held_ = 0;
+};
+
 class Engine {
  public:
-  explicit Engine(const EngineConfigHost &cfg);
+  // STREAM: the caller's stream, or null for a stream of the engine's own.
+  explicit Engine(const EngineConfigHost &cfg, cudaStream_t stream = nullptr);
   ~Engine();
 
   uint32_t add_scene(SceneImpl *scene);                 // returns slot; throws
+  // Forget every scene (slots restart at 0).  Only while nothing is in flight.
+  void reset_scenes();
+  bool idle() const { return jobs_.empty(); }
+  cudaStream_t stream() const { return stream_; }
+  const EngineConfigHost &config() const { return cfg_; }
+  // Per-kernel device time (CUDA events around each kernel instead of graph
+  // launches) while profiling is on.
+  struct Profile {
+    double closest_ms = 0, shadow_ms = 0, shade_ms = 0, other_ms = 0;
+    uint64_t iterations = 0;
+  };
+  void set_profile(bool on) { profile_on_ = on; }
+  const Profile &profile() const { return prof_; }
+  void clear_counters();
   // Queue a job; OUT is a host (on_device = false) or device image buffer.
   // SUBMIT_MS (engine clock) overrides the submission time recorded.
   uint64_t submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRenderParams &p, float *out,
@@ -102,8 +136,8 @@ class Engine {
   // Returns false when there is nothing in flight and nothing pending.
   bool step();
   JobStatsHost stats(uint64_t job);
-  uint64_t rays_closest() const { return last_ctl_.rays_closest; }
-  uint64_t rays_shadow() const { return last_ctl_.rays_shadow; }
+  uint64_t rays_closest() const { return last_ctl_.rays_closest - base_closest_; }
+  uint64_t rays_shadow() const { return last_ctl_.rays_shadow - base_shadow_; }
   double now_ms() const;
   uint32_t launches() const { return kernel_launches_; }
 
@@ -124,18 +158,23 @@ class Engine {
     float *wsum = nullptr;
     float *dev_out = nullptr;
     uint64_t bytes = 0;
-    bool canceled = false;
+    bool canceled = false, cancel_sent = false;
     JobStatsHost st;
   };
 
   void build_graph();
+  void launch_iterations();
   void admit();
   void push_items();
-  void finish_job(HostJob &j);
   void release_job(HostJob &j);
+  void *stage(const void *src, size_t n);   // copy into this step's pinned staging area
 
   EngineConfigHost cfg_;
   cudaStream_t stream_ = nullptr;
+  bool own_stream_ = false;
+  bool profile_on_ = false;
+  Profile prof_;
+  std::vector<cudaEvent_t> events_;
   cudaGraphExec_t graph_ = nullptr;
   int graph_stack_ = 0;
   // device buffers
@@ -151,8 +190,11 @@ class Engine {
   EngineJobDev *jobs_dev_;
   unsigned long long *job_done_;
   DevScene *scenes_dev_;
-  uint32_t max_scenes_ = 64;
+  uint32_t max_scenes_ = 0;
   // host mirrors
+  BlockCache cache_;
+  char *staging_ = nullptr;                    // pinned, reused every step
+  size_t staging_cap_ = 0, staging_used_ = 0;
   EngineCtl *ctl_host_ = nullptr;              // pinned
   unsigned long long *done_host_ = nullptr;    // pinned
   EngineCtl last_ctl_{};
@@ -167,6 +209,7 @@ class Engine {
   uint64_t budget_used_ = 0;
   size_t rr_ = 0;
   uint32_t kernel_launches_ = 0;
+  uint64_t base_closest_ = 0, base_shadow_ = 0;
   std::chrono::steady_clock::time_point t0_;
 };
 

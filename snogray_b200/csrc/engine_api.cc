@@ -5,7 +5,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -51,8 +53,97 @@ EngineConfigHost to_host(const SnogEngineConfig *c) {
   h.max_jobs = c->max_jobs;
   h.max_lights = c->max_lights;
   h.iters_per_launch = c->iters_per_launch;
+  h.max_scenes = c->max_scenes;
   h.mem_budget = c->mem_budget;
   return h;
+}
+
+void to_abi(const EngineConfigHost &h, SnogEngineConfig *c) {
+  c->slots = h.slots;
+  c->item_paths = h.item_paths;
+  c->ring_items = h.ring_items;
+  c->max_jobs = h.max_jobs;
+  c->max_lights = h.max_lights;
+  c->iters_per_launch = h.iters_per_launch;
+  c->max_scenes = h.max_scenes;
+  c->reserved = 0;
+  c->mem_budget = h.mem_budget;
+}
+
+void check_jobs(SnogScene *const *scenes, const SnogCamera *cameras, const SnogRenderParams *params,
+                uint32_t n_jobs, float *const *outs) {
+  if (n_jobs && (!scenes || !cameras || !params)) throw Error{SNOG_EINVAL, "null argument"};
+  for (uint32_t i = 0; i < n_jobs; i++) {
+    if (!scenes[i]) throw Error{SNOG_EINVAL, "null scene"};
+    if (outs && !outs[i]) throw Error{SNOG_EINVAL, "null output buffer"};
+  }
+}
+
+uint64_t job_paths(const SnogRenderParams &p) { return uint64_t(p.width + 4) * (p.height + 4) * p.spp; }
+
+// Defaults sized to a batch: no more queue slots than the batch has paths,
+// shadow queue for the most light samples any job takes, a job slot per job.
+EngineConfigHost auto_config(SnogScene *const *scenes, const SnogRenderParams *params, uint32_t n_jobs) {
+  EngineConfigHost h;
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n_jobs; i++) total += job_paths(params[i]);
+  while (h.slots > 65536 && uint64_t(h.slots) / 2 >= total) h.slots /= 2;
+  uint32_t ml = 1;
+  std::unordered_map<SceneImpl *, int> distinct;
+  for (uint32_t i = 0; i < n_jobs; i++) {
+    ml = std::max(ml, scenes[i]->impl->dev.n_lights * std::max(1u, params[i].direct_samples));
+    distinct[scenes[i]->impl] = 1;
+  }
+  h.max_lights = ml;
+  h.max_jobs = std::max<uint32_t>(h.max_jobs, std::min<uint32_t>(n_jobs, 1u << 16));
+  h.max_scenes = std::max<uint32_t>(h.max_scenes, uint32_t(distinct.size()));
+  return h;
+}
+
+bool profile_requested() {
+  const char *e = std::getenv("SNOG_PROFILE_KERNELS");
+  return e && e[0] == '1';
+}
+
+// Render a batch to completion on an idle engine.
+void render_on(Engine &eng, SnogScene *const *scenes, const SnogCamera *cameras, const SnogRenderParams *params,
+               uint32_t n_jobs, float *const *outs, bool outs_on_device, SnogBatchStats *stats) {
+  if (!eng.idle()) throw Error{SNOG_EBUSY, "engine has jobs in flight"};
+  eng.reset_scenes();
+  eng.clear_counters();
+  eng.set_profile(profile_requested());
+  std::unordered_map<SceneImpl *, uint32_t> slot_of;
+  for (uint32_t i = 0; i < n_jobs; i++) {
+    SceneImpl *si = scenes[i]->impl;
+    if (!slot_of.count(si)) slot_of[si] = eng.add_scene(si);
+  }
+  const double t0 = eng.now_ms();
+  uint64_t paths = 0;
+  std::vector<uint64_t> ids(n_jobs);
+  for (uint32_t i = 0; i < n_jobs; i++) {
+    ids[i] = eng.submit(slot_of[scenes[i]->impl], cameras[i], params[i], outs ? outs[i] : nullptr,
+                        outs ? outs_on_device : false);
+    paths += uint64_t(params[i].width) * params[i].height * params[i].spp;
+  }
+  eng.run_to_completion();
+  for (uint32_t i = 0; i < n_jobs; i++)
+    if (eng.stats(ids[i]).status != SNOG_OK)
+      throw Error{eng.stats(ids[i]).status, "job " + std::to_string(i) + " could not be rendered (device memory)"};
+  if (stats) {
+    std::memset(stats, 0, sizeof *stats);
+    stats->paths = paths;
+    stats->closest_rays = eng.rays_closest();
+    stats->shadow_rays = eng.rays_shadow();
+    stats->wall_ms = eng.now_ms() - t0;
+    stats->kernel_launches = eng.launches();
+    const Engine::Profile &pr = eng.profile();
+    stats->iterations = uint32_t(pr.iterations);
+    stats->closest_ms = pr.closest_ms;
+    stats->shadow_ms = pr.shadow_ms;
+    stats->shade_ms = pr.shade_ms;
+    stats->other_ms = pr.other_ms;
+  }
+  eng.set_profile(false);
 }
 
 void fill(SnogJobStats *o, const JobStatsHost &s) {
@@ -65,6 +156,11 @@ void fill(SnogJobStats *o, const JobStatsHost &s) {
 }
 
 }  // namespace
+
+struct SnogEngine {
+  std::unique_ptr<Engine> engine;
+  std::mutex mu;
+};
 
 struct SnogServer {
   std::unique_ptr<Engine> engine;
@@ -155,14 +251,37 @@ extern "C" {
 int snog_engine_default_config(SnogEngineConfig *cfg) {
   return api_call([&] {
     if (!cfg) throw Error{SNOG_EINVAL, "null argument"};
-    EngineConfigHost h;
-    cfg->slots = h.slots;
-    cfg->item_paths = h.item_paths;
-    cfg->ring_items = h.ring_items;
-    cfg->max_jobs = h.max_jobs;
-    cfg->max_lights = h.max_lights;
-    cfg->iters_per_launch = h.iters_per_launch;
-    cfg->mem_budget = h.mem_budget;
+    to_abi(EngineConfigHost{}, cfg);
+    return int(SNOG_OK);
+  });
+}
+
+int snog_engine_create(const SnogEngineConfig *cfg, void *stream, SnogEngine **out) {
+  return api_call([&] {
+    if (!out) throw Error{SNOG_EINVAL, "null argument"};
+    std::unique_ptr<SnogEngine> e(new SnogEngine);
+    e->engine.reset(new Engine(to_host(cfg), static_cast<cudaStream_t>(stream)));
+    *out = e.release();
+    return int(SNOG_OK);
+  });
+}
+
+int snog_engine_render(SnogEngine *engine, SnogScene *const *scenes, const SnogCamera *cameras,
+                       const SnogRenderParams *params, uint32_t n_jobs, float *const *outs, int outs_on_device,
+                       SnogBatchStats *stats) {
+  return api_call([&] {
+    if (!engine) throw Error{SNOG_EINVAL, "null argument"};
+    check_jobs(scenes, cameras, params, n_jobs, outs);
+    if (!outs && n_jobs) throw Error{SNOG_EINVAL, "null argument"};
+    std::lock_guard<std::mutex> lk(engine->mu);
+    render_on(*engine->engine, scenes, cameras, params, n_jobs, outs, outs_on_device != 0, stats);
+    return int(SNOG_OK);
+  });
+}
+
+int snog_engine_destroy(SnogEngine *engine) {
+  return api_call([&] {
+    delete engine;
     return int(SNOG_OK);
   });
 }
@@ -171,47 +290,96 @@ int snog_render_batch(SnogScene *const *scenes, const SnogCamera *cameras, const
                       uint32_t n_jobs, float *const *outs, int outs_on_device, const SnogEngineConfig *cfg,
                       SnogBatchStats *stats) {
   return api_call([&] {
-    if (n_jobs && (!scenes || !cameras || !params || !outs)) throw Error{SNOG_EINVAL, "null argument"};
-    EngineConfigHost h = to_host(cfg);
-    if (!cfg) {
-      // Size the ray queues to the batch: no more slots than paths.
-      uint64_t total = 0;
-      for (uint32_t i = 0; i < n_jobs; i++)
-        total += uint64_t(params[i].width + 4) * (params[i].height + 4) * params[i].spp;
-      while (h.slots > 65536 && uint64_t(h.slots) / 2 >= total) h.slots /= 2;
-      uint32_t ml = 1;
-      for (uint32_t i = 0; i < n_jobs; i++) {
-        if (!scenes[i]) throw Error{SNOG_EINVAL, "null scene"};
-        ml = std::max(ml, scenes[i]->impl->dev.n_lights * std::max(1u, params[i].direct_samples));
+    check_jobs(scenes, cameras, params, n_jobs, outs);
+    if (!outs && n_jobs) throw Error{SNOG_EINVAL, "null argument"};
+    Engine eng(cfg ? to_host(cfg) : auto_config(scenes, params, n_jobs));
+    render_on(eng, scenes, cameras, params, n_jobs, outs, outs_on_device != 0, stats);
+    return int(SNOG_OK);
+  });
+}
+
+// Coordinate descent over (slots, item_paths, iters_per_launch) on a sample
+// of the batch: up to SAMPLE_JOBS jobs, evenly spaced, at reduced spp so the
+// sample is a few queue-fulls of paths.  Results are discarded.
+int snog_engine_autotune(SnogScene *const *scenes, const SnogCamera *cameras, const SnogRenderParams *params,
+                         uint32_t n_jobs, uint32_t sample_jobs, const SnogEngineConfig *base,
+                         SnogEngineConfig *best, double *best_mpaths) {
+  return api_call([&] {
+    check_jobs(scenes, cameras, params, n_jobs, nullptr);
+    if (!best || n_jobs == 0) throw Error{SNOG_EINVAL, "null argument or empty batch"};
+    if (sample_jobs == 0) sample_jobs = 64;
+    const uint32_t ns = std::min(n_jobs, sample_jobs);
+    std::vector<SnogScene *> sc(ns);
+    std::vector<SnogCamera> cam(ns);
+    std::vector<SnogRenderParams> prm(ns);
+    uint64_t sample_paths = 0;
+    for (uint32_t k = 0; k < ns; k++) {
+      const uint32_t i = uint32_t(uint64_t(k) * n_jobs / ns);
+      sc[k] = scenes[i];
+      cam[k] = cameras[i];
+      prm[k] = params[i];
+      sample_paths += job_paths(prm[k]);
+    }
+    // Aim for ~48M sample paths (several fills of the largest queue tried).
+    const double target = 48.0 * (1 << 20);
+    if (sample_paths > target) {
+      const double f = target / double(sample_paths);
+      sample_paths = 0;
+      for (auto &p : prm) {
+        p.spp = std::max(1u, uint32_t(p.spp * f));
+        sample_paths += job_paths(p);
       }
-      h.max_lights = ml;
-      if (h.max_jobs < n_jobs) h.max_jobs = n_jobs;
     }
-    Engine eng(h);
-    std::unordered_map<SceneImpl *, uint32_t> slot_of;
-    for (uint32_t i = 0; i < n_jobs; i++) {
-      if (!scenes[i]) throw Error{SNOG_EINVAL, "null scene"};
-      SceneImpl *si = scenes[i]->impl;
-      if (!slot_of.count(si)) slot_of[si] = eng.add_scene(si);
+    EngineConfigHost cur = base ? to_host(base) : auto_config(scenes, params, n_jobs);
+    {
+      EngineConfigHost need = auto_config(scenes, params, n_jobs);
+      cur.max_lights = std::max(cur.max_lights, need.max_lights);
+      cur.max_scenes = std::max(cur.max_scenes, need.max_scenes);
+      cur.max_jobs = std::max(cur.max_jobs, ns);
     }
-    const double t0 = eng.now_ms();
     uint64_t paths = 0;
-    std::vector<uint64_t> ids(n_jobs);
-    for (uint32_t i = 0; i < n_jobs; i++) {
-      ids[i] = eng.submit(slot_of[scenes[i]->impl], cameras[i], params[i], outs[i], outs_on_device != 0);
-      paths += uint64_t(params[i].width) * params[i].height * params[i].spp;
+    for (auto &p : prm) paths += uint64_t(p.width) * p.height * p.spp;
+    std::vector<std::vector<float>> imgs(ns);
+    std::vector<float *> outs(ns);
+    for (uint32_t k = 0; k < ns; k++) {
+      imgs[k].resize(size_t(prm[k].width) * prm[k].height * 3);
+      outs[k] = imgs[k].data();
     }
-    eng.run_to_completion();
-    for (uint32_t i = 0; i < n_jobs; i++)
-      if (eng.stats(ids[i]).status != SNOG_OK)
-        throw Error{eng.stats(ids[i]).status, "job " + std::to_string(i) + " could not be rendered (device memory)"};
-    if (stats) {
-      stats->paths = paths;
-      stats->closest_rays = eng.rays_closest();
-      stats->shadow_rays = eng.rays_shadow();
-      stats->wall_ms = eng.now_ms() - t0;
-      stats->kernel_launches = eng.launches();
-    }
+    auto measure = [&](const EngineConfigHost &h) {
+      Engine eng(h);
+      SnogBatchStats st;
+      render_on(eng, sc.data(), cam.data(), prm.data(), ns, outs.data(), false, &st);   // warm (graph, caches)
+      render_on(eng, sc.data(), cam.data(), prm.data(), ns, outs.data(), false, &st);
+      return double(paths) / (st.wall_ms * 1e3);
+    };
+    double best_rate = measure(cur);
+    auto try_values = [&](uint32_t EngineConfigHost::*field, std::initializer_list<uint32_t> values) {
+      const uint32_t keep = cur.*field;
+      uint32_t best_v = keep;
+      for (uint32_t v : values) {
+        if (v == keep) continue;
+        EngineConfigHost h = cur;
+        h.*field = v;
+        if (field == &EngineConfigHost::slots && v / 2 > sample_paths) continue;
+        double r;
+        try {
+          r = measure(h);
+        } catch (const Error &e) {
+          if (e.code == SNOG_ENOMEM) continue;
+          throw;
+        }
+        if (r > best_rate * 1.02) {
+          best_rate = r;
+          best_v = v;
+        }
+      }
+      cur.*field = best_v;
+    };
+    try_values(&EngineConfigHost::slots, {1u << 21, 1u << 22, 1u << 23, 1u << 24});
+    try_values(&EngineConfigHost::item_paths, {1u << 12, 1u << 14, 1u << 16, 1u << 18});
+    try_values(&EngineConfigHost::iters_per_launch, {1u, 2u, 4u, 8u});
+    to_abi(cur, best);
+    if (best_mpaths) *best_mpaths = best_rate;
     return int(SNOG_OK);
   });
 }

@@ -126,12 +126,15 @@ extern "C" int snog_render_device_noalloc(SnogScene *scene, const SnogCamera *ca
       throw Error{SNOG_EINVAL, "octree deeper than the traversal kernels support (84 levels)"};
     // Path capacity of the wave region, in whole pixels' worth of samples.
     const size_t wave_bytes = kScratchBytes - kAccumBytes - 32 * 256;   // per-array alignment slack
-    uint64_t cap = wave_bytes / wave_bytes_per_path(S.dev.n_lights);
+    if (p.direct_samples > 64) throw Error{SNOG_EINVAL, "direct_samples must be <= 64"};
+    // Shadow-queue entries a vertex may need: two per light sample.
+    const uint32_t ls = (S.dev.n_lights ? S.dev.n_lights : 1u) * (p.direct_samples ? p.direct_samples : 1u);
+    uint64_t cap = wave_bytes / wave_bytes_per_path(ls);
     cap = (cap / p.spp) * p.spp;
     if (cap < p.spp)
       throw Error{SNOG_EINVAL, std::to_string(p.spp) + " samples per pixel do not fit the no-alloc scratch "
-                                   "for this scene's " + std::to_string(S.dev.n_lights) +
-                                   " lights; use snog_render_device"};
+                                   "for this scene's " + std::to_string(ls) +
+                                   " light samples per vertex; use snog_render_device"};
     const uint64_t total = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
     if (cap > total) cap = total;
 
@@ -140,7 +143,7 @@ extern "C" int snog_render_device_noalloc(SnogScene *scene, const SnogCamera *ca
     float4 *accum = reinterpret_cast<float4 *>(base);
     float *wsum = reinterpret_cast<float *>(base + kMaxPixels * 16);
     WaveBuffers wb;
-    carve_waves(wb, base + kAccumBytes, kScratchBytes - kAccumBytes, cap, S.dev.n_lights);
+    carve_waves(wb, base + kAccumBytes, kScratchBytes - kAccumBytes, cap, ls);
     JobConsts jc = make_job(S.dev, *camera, p);
     uint32_t waves = 0, launches = 0;
     cudaError_t e = render_job(S.dev, jc, wb, accum, wsum, d_out_rgb, cudaStream_t(stream), &waves, &launches);

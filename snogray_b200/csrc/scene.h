@@ -23,7 +23,6 @@ struct RenderCache {
   float *wsum = nullptr;       // W*H filter weight sums
   float *out = nullptr;        // W*H*3 resolved image (host-output calls)
   size_t npix_cap = 0;
-  uint32_t *trace_scratch = nullptr;   // ray-batch dispenser counter (+ flags)
   void release();
 };
 
@@ -47,8 +46,18 @@ struct SceneImpl {
   // host copies needed by the host side of rendering
   float bbox_min[3], bbox_max[3];
   bool on_device = false;
-  RenderCache rc;
+  uint32_t *trace_scratch = nullptr;   // ray-batch dispenser counter (+ flags)
 };
+
+// Working memory of the plain renderer, one per device, shared by every
+// scene: renders on any stream take it in turn, each waiting (on the device)
+// for the event the previous one recorded after its last use.
+struct RenderPool {
+  std::mutex mu;
+  RenderCache rc;
+  cudaEvent_t done = nullptr;
+};
+RenderPool &render_pool(int device);
 
 // Build and upload; throws snog::Error on failure.
 SceneImpl *build_scene(const SnogSceneDesc &desc, bool upload = true);

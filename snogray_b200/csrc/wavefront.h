@@ -28,7 +28,7 @@ struct JobConsts {
 // Device buffers for one wave of paths (sized for wave_cap paths).
 struct WaveBuffers {
   uint64_t wave_cap = 0;
-  uint32_t n_lights = 0;
+  uint32_t n_lights = 0;                     // light samples per vertex the shadow queue is sized for
   float4 *thr = nullptr, *rad = nullptr;     // per path: throughput+rr, radiance+alpha
   uint32_t *pstate = nullptr;                // per path: length, flags, media stack
   float4 *q_o[2] = {nullptr, nullptr};       // ray queues: origin + t0
@@ -44,7 +44,8 @@ struct WaveBuffers {
   void *block = nullptr;
 };
 
-// Bytes needed per path of wave capacity for a scene with n_lights lights.
+// Bytes needed per path of wave capacity when a vertex takes N_LIGHTS light
+// samples (lights x direct_samples; the shadow queue holds two rays each).
 uint64_t wave_bytes_per_path(uint32_t n_lights);
 // Allocate / free (cudaMalloc of one block).
 cudaError_t wave_alloc(WaveBuffers &wb, uint64_t cap, uint32_t n_lights);

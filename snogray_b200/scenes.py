@@ -376,7 +376,7 @@ def terrain_params(width=1920, height=1080, spp=64, seed=0):
 # Random-soup scene with mixed materials and one area light, for the batched
 # and served workloads.
 
-def soup_scene(n_tris, seed, envmap=None):
+def soup_scene(n_tris, seed, envmap=None, area_light=True):
     rng = np.random.default_rng(seed)
     recs = [material(MAT_LAMBERT, rng.uniform(0.2, 0.8, 3)),
             material(MAT_COOK_TORRANCE, rng.uniform(0.2, 0.8, 3), (1, 1, 1),
@@ -386,9 +386,10 @@ def soup_scene(n_tris, seed, envmap=None):
     # Lambert/Cook-Torrance mix: parts must be contiguous runs.
     n_ct = int(rng.uniform(0.2, 0.8) * n_tris)
     s.tri_mat = np.concatenate([np.zeros(n_tris - n_ct, np.uint32), np.ones(n_ct, np.uint32)])
-    tp = np.zeros(1, TRIPAR_DTYPE)
-    tp[0] = ((0.35, 0.35, 1.3), (0.3, 0, 0), (0, 0.3, 0), 1, 2)   # faces -z
-    s.tripars = tp
+    if area_light or envmap is None:
+        tp = np.zeros(1, TRIPAR_DTYPE)
+        tp[0] = ((0.35, 0.35, 1.3), (0.3, 0, 0), (0, 0.3, 0), 1, 2)   # faces -z
+        s.tripars = tp
     if envmap is not None:
         s.envmap = envmap
     s.name = f"soup{n_tris}_s{seed}"
@@ -405,3 +406,73 @@ def orbit_camera(width, height, rng, center=(0.5, 0.5, 0.5), dist=1.8):
     cam.point(center, (0, 0, 1))
     cam.set_vert_fov(math.radians(50.0), width / height)
     return cam
+
+
+# ---------------------------------------------------------------------------
+# Batched workload: many independent small scenes of uneven size rendered
+# together (1024 random-triangle soups of 1k-50k triangles, log-uniform, a
+# Lambert/Cook-Torrance mix and one area light each; resolution from
+# {64, 128, 256}^2, spp from {4, 16, 64}).
+
+BATCH_RES = (64, 128, 256)
+BATCH_SPP = (4, 16, 64)
+
+
+def batch_workload(n_jobs=1024, seed=4, tri_lo=1000, tri_hi=50000):
+    """[(SceneData, Camera, RenderParams)] for the batched workload."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(n_jobs):
+        n = int(round(math.exp(rng.uniform(math.log(tri_lo), math.log(tri_hi)))))
+        res = int(rng.choice(BATCH_RES))
+        spp = int(rng.choice(BATCH_SPP))
+        sd = soup_scene(n, seed=10000 + k)
+        cam = orbit_camera(res, res, rng)
+        jobs.append((sd, cam, RenderParams(res, res, spp, seed=k)))
+    return jobs
+
+
+# ---------------------------------------------------------------------------
+# Serving workload: 8 resident scenes of 10k-8M random triangles (mixed
+# materials; area light, or a sky envmap for every other scene) and a stream
+# of requests at Poisson arrivals, each a random scene, a camera on a sphere
+# around it, a resolution from {128, 256, 512, 1024}^2 and spp from {4, 16, 64}.
+
+SERVE_SIZES = (10_000, 50_000, 200_000, 1_000_000, 2_000_000, 4_000_000, 6_000_000, 8_000_000)
+SERVE_RES = (128, 256, 512, 1024)
+SERVE_SPP = (4, 16, 64)
+
+
+def serve_scenes(sizes=SERVE_SIZES, seed=21):
+    env = sky_envmap(256, 128, sigma_deg=3.0, peak=200.0)
+    out = []
+    for k, n in enumerate(sizes):
+        if k % 2:
+            out.append(soup_scene(n, seed=seed + k, envmap=env, area_light=False))
+        else:
+            out.append(soup_scene(n, seed=seed + k))
+    return out
+
+
+@dataclass
+class Request:
+    arrival_s: float
+    scene: int
+    camera: Camera
+    params: RenderParams
+
+
+def serve_requests(n=2000, rate=200.0, n_scenes=len(SERVE_SIZES), seed=22,
+                   res_choices=SERVE_RES, spp_choices=SERVE_SPP):
+    """N requests with exponential inter-arrival times at RATE per second."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    t -= t[0]
+    reqs = []
+    for k in range(n):
+        res = int(rng.choice(res_choices))
+        spp = int(rng.choice(spp_choices))
+        sc = int(rng.integers(n_scenes))
+        cam = orbit_camera(res, res, rng)
+        reqs.append(Request(float(t[k]), sc, cam, RenderParams(res, res, spp, seed=k)))
+    return reqs

@@ -28,7 +28,7 @@ def _jobs():
     return [
         (cornell, scenes.cornell_camera(48, 40), scenes.cornell_params(48, 40, 8, seed=3)),
         (terrain, scenes.terrain_camera(64, 36), scenes.terrain_params(64, 36, 4, seed=4)),
-        (soup, scenes.orbit_camera(40, 40, rng), sb.RenderParams(40, 40, 16, 3, 8, 1, seed=5)),
+        (soup, scenes.orbit_camera(40, 40, rng), sb.RenderParams(40, 40, 16, 3, 8, 2, seed=5)),
         (cornell, scenes.cornell_camera(32, 32), scenes.cornell_params(32, 32, 16, seed=6)),
     ]
 
@@ -103,3 +103,58 @@ def test_server_cancel_and_timeouts():
         assert e.value.code == sb.SNOG_ETIMEOUT
         img, st = srv.wait(j, timeout_ms=120000)
         assert st["status"] == 0
+
+
+def test_persistent_engine_reuse_and_device_outputs():
+    import torch
+    jobs = _jobs()
+    with sb.Engine(sb.engine_config(slots=1 << 18, item_paths=1 << 13)) as eng:
+        a, st_a = eng.render(jobs)
+        b, st_b = eng.render(jobs[::-1])          # other scene slots, same images
+        outs = [torch.empty((p.height, p.width, 3), dtype=torch.float32, device="cuda") for _, _, p in jobs]
+        none, st_c = eng.render(jobs, device_outs=[o.data_ptr() for o in outs])
+        torch.cuda.synchronize()
+    assert none is None
+    assert st_a["paths"] == st_b["paths"] == st_c["paths"]
+    for k, (sc, cam, p) in enumerate(jobs):
+        ref, _ = sc.render(cam, p)
+        assert np.allclose(a[k], ref, rtol=RTOL, atol=ATOL)
+        assert np.allclose(b[len(jobs) - 1 - k], ref, rtol=RTOL, atol=ATOL)
+        assert np.allclose(outs[k].cpu().numpy(), ref, rtol=RTOL, atol=ATOL)
+
+
+def test_profiled_batch_reports_kernel_times(monkeypatch):
+    jobs = _jobs()[:2]
+    monkeypatch.setenv("SNOG_PROFILE_KERNELS", "1")
+    imgs, st = sb.render_batch(jobs)
+    assert st["iterations"] > 0 and st["closest_ms"] > 0 and st["shadow_ms"] > 0 and st["shade_ms"] > 0
+    for (sc, cam, p), img in zip(jobs, imgs):
+        ref, _ = sc.render(cam, p)
+        assert np.allclose(img, ref, rtol=RTOL, atol=ATOL)
+
+
+def test_autotune_returns_a_working_config():
+    jobs = _jobs()
+    cfg, rate = sb.autotune(jobs, sample_jobs=4)
+    assert rate > 0
+    assert cfg.slots >= 1024 and cfg.item_paths > 0 and cfg.iters_per_launch > 0
+    imgs, _ = sb.render_batch(jobs, cfg)
+    for (sc, cam, p), img in zip(jobs, imgs):
+        ref, _ = sc.render(cam, p)
+        assert np.allclose(img, ref, rtol=RTOL, atol=ATOL)
+
+
+def test_many_scenes_in_one_batch():
+    """More distinct scenes than jobs slots of the default table size: a
+    uneven batch of small soups (the batched workload in miniature)."""
+    rng = np.random.default_rng(9)
+    jobs = []
+    for k in range(40):
+        n = int(rng.integers(200, 3000))
+        res = int(rng.choice([16, 24, 32]))
+        jobs.append((sb.Scene(scenes.soup_scene(n, 100 + k)), scenes.orbit_camera(res, res, rng),
+                     sb.RenderParams(res, res, int(rng.choice([1, 4, 8])), seed=k)))
+    imgs, st = sb.render_batch(jobs, sb.engine_config(slots=1 << 14, item_paths=512, max_scenes=64))
+    for (sc, cam, p), img in zip(jobs, imgs):
+        ref, _ = sc.render(cam, p)
+        assert np.allclose(img, ref, rtol=RTOL, atol=ATOL)

@@ -63,6 +63,24 @@ def workload():
     return sd, cam
 
 
+def max_over_ranks(x, dist=None):
+    """Max of X over the ranks of the default process group (X itself when
+    DIST is None): the job's time is its slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank):
+    """Each rank renders its own replica of the job with its own sample
+    streams (weak scaling: the whole job's paths = ranks x paths per rank)."""
+    return 1 + rank
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -393,16 +411,9 @@ def bench_ours(args):
         if pg is not None:
             pg.barrier()
 
-    def max_over_ranks(x):
-        if pg is None:
-            return x
-        t = torch.tensor([x], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
-
     sd, cam = workload()
     scene = sb.Scene(sd)
-    params = scenes.terrain_params(WIDTH, HEIGHT, SPP, seed=1 + rank)
+    params = scenes.terrain_params(WIDTH, HEIGHT, SPP, seed=replica_seed(rank))
     job = [(scene, cam, params)]
     out = torch.empty((HEIGHT, WIDTH, 3), dtype=torch.float32, device="cuda")
     stream = torch.cuda.Stream()
@@ -410,7 +421,12 @@ def bench_ours(args):
     paths_per_step = WIDTH * HEIGHT * SPP
 
     # ---- engine configuration picked by the autotuner ----------------------
-    cfg, _ = sb.autotune(job, sample_jobs=1)
+    if args.no_autotune:
+        cfg = sb.engine_config(max_lights=max(1, scene.info()["n_lights"]))
+        if args.slots:
+            cfg.slots = args.slots
+    else:
+        cfg, _ = sb.autotune(job, sample_jobs=1)
     eng = sb.Engine(cfg, stream=sptr)
 
     def step():
@@ -439,7 +455,7 @@ def bench_ours(args):
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
-    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, pg)
     value = paths_per_step * ws / ms * 1e-3          # Mpaths/s, whole job
 
     # ---- the plain renderer (one job per launch sequence) on the same job --
@@ -451,7 +467,7 @@ def bench_ours(args):
         scene.render_device(cam, params, out.data_ptr(), sptr)
     e1.record(stream)
     torch.cuda.synchronize()
-    plain_ms = max_over_ranks(e0.elapsed_time(e1) / n_plain)
+    plain_ms = max_over_ranks(e0.elapsed_time(e1) / n_plain, pg)
 
     # ---- per-kernel times for the roofline (live, CUDA events) ------------
     os.environ["SNOG_PROFILE_KERNELS"] = "1"
@@ -466,7 +482,7 @@ def bench_ours(args):
     n_e2e = max(1, args.steps)
     for _ in range(n_e2e):
         eng.render(job, host_outs=[host])
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / n_e2e)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / n_e2e, pg)
     e2e_value = paths_per_step * ws / e2e_s * 1e-6
     h2d = ctypes.sizeof(sb.SnogCamera) + ctypes.sizeof(sb.SnogRenderParams)
     d2h = WIDTH * HEIGHT * 3 * 4
@@ -565,6 +581,9 @@ def main():
     ap.add_argument("--isec-only", action="store_true",
                     help="only the intersection-only batch (1M triangles, 16M rays)")
     ap.add_argument("--isec-rays", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default engine configuration (profiling runs)")
+    ap.add_argument("--slots", type=int, default=0, help="engine queue slots with --no-autotune")
     ap.add_argument("--batch-jobs", type=int, default=1024,
                     help="jobs of the batched workload (0 = skip it)")
     ap.add_argument("--serve-requests", type=int, default=200,

@@ -101,28 +101,18 @@ __global__ void __launch_bounds__(128, 6) k_e_closest(EngineCtl *ctl, uint32_t c
                                                       float *hit_t) {
   const uint32_t n = ctl->qcount[cur];
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_closest += n;
-  Traversal<STACK> tr;
-  RayDispenser disp;
-  uint32_t ray = RayDispenser::kIdle;
-  const DevScene *sc = scenes;
   TraceCounters c{0, 0, 0};
-  for (;;) {
-    bool all_idle;
-    const uint32_t got =
-        disp.fetch(&ctl->disp_closest, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
-    if (all_idle) break;
-    if (got != RayDispenser::kIdle) {
-      ray = got;
-      sc = scenes + jobs[q.meta[ray].y].scene;
-      const float4 o = q.o[ray], d = q.d[ray];
-      tr.init(*sc, xyz(o), xyz(d), o.w, d.w);
-    }
-    if (ray == RayDispenser::kIdle) continue;
-    if (!tr.template step<false>(*sc, c)) continue;
-    hit_ref[ray] = tr.hit_ref;
-    hit_t[ray] = tr.t1;
-    ray = RayDispenser::kIdle;
-  }
+  trace_loop<STACK>(
+      &ctl->disp_closest, n, c,
+      [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
+        const float4 o = q.o[ray], d = q.d[ray];
+        tr.init(scenes[jobs[q.meta[ray].y].scene], xyz(o), xyz(d), o.w, d.w);
+        any = false;
+      },
+      [&](uint32_t ray, Traversal<STACK> &tr, bool) {
+        hit_ref[ray] = tr.hit_ref;
+        hit_t[ray] = tr.t1;
+      });
   if (c.overflow) atomicOr(&ctl->err, 1u);
 }
 
@@ -130,33 +120,22 @@ template <int STACK>
 __global__ void __launch_bounds__(128, 6) k_e_shadow(EngineCtl *ctl, const DevScene *scenes, ESQ q) {
   const uint32_t n = ctl->scount;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_shadow += n;
-  Traversal<STACK> tr;
-  RayDispenser disp;
-  uint32_t ray = RayDispenser::kIdle;
-  const DevScene *sc = scenes;
   TraceCounters c{0, 0, 0};
-  for (;;) {
-    bool all_idle;
-    const uint32_t got =
-        disp.fetch(&ctl->disp_shadow, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
-    if (all_idle) break;
-    if (got != RayDispenser::kIdle) {
-      ray = got;
-      sc = scenes + __float_as_uint(q.c[ray].w);
-      const float4 o = q.o[ray], d = q.d[ray];
-      tr.init(*sc, xyz(o), xyz(d), o.w, d.w);
-    }
-    if (ray == RayDispenser::kIdle) continue;
-    if (!tr.template step<true>(*sc, c)) continue;
-    if (tr.hit_ref == PREF_END) {
-      const float4 cc = q.c[ray];
-      float *dst = reinterpret_cast<float *>(q.tgt[ray]);
-      atomicAdd(dst, cc.x);
-      atomicAdd(dst + 1, cc.y);
-      atomicAdd(dst + 2, cc.z);
-    }
-    ray = RayDispenser::kIdle;
-  }
+  trace_loop<STACK>(
+      &ctl->disp_shadow, n, c,
+      [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
+        const float4 o = q.o[ray], d = q.d[ray];
+        tr.init(scenes[__float_as_uint(q.c[ray].w)], xyz(o), xyz(d), o.w, d.w);
+        any = true;
+      },
+      [&](uint32_t ray, Traversal<STACK> &tr, bool) {
+        if (tr.hit_ref != PREF_END) return;
+        const float4 cc = q.c[ray];
+        float *dst = reinterpret_cast<float *>(q.tgt[ray]);
+        atomicAdd(dst, cc.x);
+        atomicAdd(dst + 1, cc.y);
+        atomicAdd(dst + 2, cc.z);
+      });
   if (c.overflow) atomicOr(&ctl->err, 1u);
 }
 

@@ -19,27 +19,17 @@ __global__ void __launch_bounds__(128) k_trace_batch(DevScene s, const float *__
                                                      unsigned long long *__restrict__ counters,
                                                      uint32_t *__restrict__ err, uint32_t *__restrict__ fetch) {
   unsigned long long cn = 0, ct = 0, an = 0, at = 0;
-  Traversal<STACK> tr;
-  RayDispenser disp;
-  uint32_t ray = RayDispenser::kIdle;
-  TraceCounters c{0, 0, 0};
-  for (;;) {
-    bool all_idle;
-    const uint32_t got = disp.fetch(fetch, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
-    if (all_idle) break;
-    if (got != RayDispenser::kIdle) {
-      ray = got;
-      tr.init(s, f3(rays[ray], rays[size_t(n) + ray], rays[2 * size_t(n) + ray]),
-              f3(rays[3 * size_t(n) + ray], rays[4 * size_t(n) + ray], rays[5 * size_t(n) + ray]), 0.f,
-              rays[6 * size_t(n) + ray]);
-      c = TraceCounters{0, 0, 0};
-    }
-    if (ray == RayDispenser::kIdle) continue;
-    const bool closest = ray < n_closest;
-    const bool fin = closest ? tr.template step<false>(s, c) : tr.template step<true>(s, c);
-    if (!fin) continue;
-    const uint32_t i = ray, ref = tr.hit_ref;
-    ray = RayDispenser::kIdle;
+  TraceCounters c{0, 0, 0}, base{0, 0, 0};
+  auto start = [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
+    tr.init(s, f3(rays[ray], rays[size_t(n) + ray], rays[2 * size_t(n) + ray]),
+            f3(rays[3 * size_t(n) + ray], rays[4 * size_t(n) + ray], rays[5 * size_t(n) + ray]), 0.f,
+            rays[6 * size_t(n) + ray]);
+    any = ray >= n_closest;
+    base = c;
+  };
+  auto done = [&](uint32_t i, Traversal<STACK> &tr, bool any) {
+    const bool closest = !any;
+    const uint32_t ref = tr.hit_ref;
     prim[i] = prim_id_of(s, ref);
     if (tout) tout[i] = (closest && ref != PREF_END) ? tr.t1 : 0.f;
     if (nrm) {
@@ -62,15 +52,16 @@ __global__ void __launch_bounds__(128) k_trace_batch(DevScene s, const float *__
       nrm[3 * size_t(i) + 1] = nv.y;
       nrm[3 * size_t(i) + 2] = nv.z;
     }
-    if (c.overflow) atomicOr(err, 1u);
     if (closest) {
-      cn += c.nodes;
-      ct += c.tests;
+      cn += c.nodes - base.nodes;
+      ct += c.tests - base.tests;
     } else {
-      an += c.nodes;
-      at += c.tests;
+      an += c.nodes - base.nodes;
+      at += c.tests - base.tests;
     }
-  }
+  };
+  trace_loop<STACK>(fetch, n, c, start, done);
+  if (c.overflow) atomicOr(err, 1u);
   if (counters) {
     // All lanes reach this point: reduce per warp, one atomic per warp.
     for (int off = 16; off > 0; off >>= 1) {

@@ -194,14 +194,14 @@ __device__ __forceinline__ bool gate_open(uint32_t cb, float t0, float t1, float
 }
 
 // A resumable octree walk for one ray.  init() sets up the root's slab
-// bounds (space/octree.cc:119-135); each step() processes one octree entry --
-// the child entered last, else the top of the stack -- exactly as one call of
-// the reference's recursive function does: parent gate, slab cull, the
-// node's surface list, then the children.  Kernels interleave the steps of
-// many rays per warp and refill lanes whose ray has finished.
-// ANY = stop at the first hit (Space::intersects / occludes).  STACK entries
-// must cover 3 * depth + 2 (chosen by the host from the tree depth); if they
-// do not, cnt.overflow is set and the result must be discarded.
+// bounds (space/octree.cc:119-135); node_step() processes one octree entry --
+// the child entered last, else the top of the stack -- as one call of the
+// reference's recursive function does: parent gate, slab cull, then the
+// node's surface list (left pending in [lp, lend) for list_round) and the
+// children.  Kernels interleave the steps of many rays per warp and refill
+// lanes whose ray has finished.  STACK entries must cover 3 * depth + 2
+// (chosen by the host from the tree depth); if they do not, cnt.overflow is
+// set and the result must be discarded.
 template <int STACK>
 struct Traversal {
   float3 o, d, lo, hi;
@@ -210,6 +210,9 @@ struct Traversal {
   uint32_t lp, lend;         // surface list still to test: plist[lp, lend)
   int sp;
   bool have;                 // a current entry (node/gate/lo/hi) is set
+  const uint4 *nodes;        // the ray's scene
+  const uint32_t *plist;
+  const float4 *prims;
   StackEntry stk[STACK];
 
   __device__ __forceinline__ void init(const DevScene &s, float3 o_, float3 d_, float t0_, float t1_) {
@@ -223,6 +226,9 @@ struct Traversal {
     gate = 0;
     lp = lend = 0;
     have = s.n_nodes != 0;
+    nodes = s.nodes;
+    plist = s.plist;
+    prims = s.prims;
     float inv = (d.x == 0.f) ? 1e9f : __fdiv_rn(1.0f, d.x);
     float a = __fmul_rn(__fsub_rn(s.origin[0], o.x), inv);
     float b = __fmul_rn(__fadd_rn(__fsub_rn(s.origin[0], o.x), s.size), inv);
@@ -241,53 +247,20 @@ struct Traversal {
     octant = (d.x >= 0.f ? 0u : 4u) | (d.y >= 0.f ? 0u : 2u) | (d.z >= 0.f ? 0u : 1u);
   }
 
-  // One unit of work: the next surface of the pending list if any, else one
-  // octree entry (the child entered last, else the top of the stack).
-  // Returns true when the walk is over (hit_ref / t1 final).
+  // The walk is over: no list pending, no current entry, empty stack.
+  __device__ __forceinline__ bool finished() const { return lp >= lend && !have && sp == 0; }
+
+  // One octree entry (call only with no list pending and !finished()).
   //
   // An entry is processed as one call of the reference's recursive function:
   // parent gate, slab cull, then the node's surface list, then its children.
   // Here the qualifying children are pushed when the node is visited and its
-  // list is tested in the following steps; the push uses the ray's extent
-  // before those tests, which only admits more children (the ray can only
-  // shrink), and every entry's gate and cull are evaluated again when it is
-  // entered -- so the tests and their order are the reference's.
-  template <bool ANY>
-  __device__ __forceinline__ bool step(const DevScene &s, TraceCounters &cnt) {
-    if (lp < lend) {
-      // Up to four surfaces of the list per step: one 128-bit load of ids
-      // (lists are 4-aligned), all records fetched before the first test,
-      // then tested in list order.
-      const uint4 ids = __ldg(reinterpret_cast<const uint4 *>(s.plist + lp));
-      const uint32_t nv = lend - lp < 4u ? lend - lp : 4u;
-      lp += 4;
-      cnt.tests += nv;
-      // Two records in flight: the next one is fetched while this one is
-      // tested (keeps live registers, and so occupancy, in check).
-      PrimRec ra = load_prim(s, ids.x);
-      PrimRec rb = load_prim(s, nv > 1 ? ids.y : ids.x);
-      if (test_prim(ra, o, d, t0, t1)) {
-        hit_ref = ids.x;
-        if (ANY) return true;
-      }
-      if (nv > 2) ra = load_prim(s, ids.z);
-      if (nv > 1 && test_prim(rb, o, d, t0, t1)) {
-        hit_ref = ids.y;
-        if (ANY) return true;
-      }
-      if (nv > 3) rb = load_prim(s, ids.w);
-      if (nv > 2 && test_prim(ra, o, d, t0, t1)) {
-        hit_ref = ids.z;
-        if (ANY) return true;
-      }
-      if (nv > 3 && test_prim(rb, o, d, t0, t1)) {
-        hit_ref = ids.w;
-        if (ANY) return true;
-      }
-      return lp >= lend && !have && sp == 0;
-    }
+  // list is tested afterwards; the push uses the ray's extent before those
+  // tests, which only admits more children (the ray can only shrink), and
+  // every entry's gate and cull are evaluated again when it is entered -- so
+  // the tests and their order are the reference's.
+  __device__ __forceinline__ void node_step(TraceCounters &cnt) {
     if (!have) {
-      if (sp == 0) return true;
       --sp;
       node = __float_as_uint(stk[sp].lo.w);
       gate = __float_as_uint(stk[sp].hi.w);
@@ -301,53 +274,148 @@ struct Traversal {
       cnt.nodes++;
       open = slab_open(t0, t1, lo, hi);
     }
-    if (open) {
-      const uint4 nd = __ldg(s.nodes + node);
-      lp = nd.z;
-      lend = nd.z + nd.w;
-      if (nd.y) {
-        const float3 half = f3(__fdiv_rn(__fsub_rn(hi.x, lo.x), 2.0f), __fdiv_rn(__fsub_rn(hi.y, lo.y), 2.0f),
-                               __fdiv_rn(__fsub_rn(hi.z, lo.z), 2.0f));
-        // Per axis the children's bounds take two values each: the near
-        // half spans [lo, lo + half], the far half [lo + half, lo + half +
-        // half] -- the same rounded sums as the reference's child ranges.
-        const float3 mid = f3(__fadd_rn(lo.x, half.x), __fadd_rn(lo.y, half.y), __fadd_rn(lo.z, half.z));
-        const float3 far = f3(__fadd_rn(mid.x, half.x), __fadd_rn(mid.y, half.y), __fadd_rn(mid.z, half.z));
-        const float3 near_lo = f3(__fadd_rn(lo.x, 0.f), __fadd_rn(lo.y, 0.f), __fadd_rn(lo.z, 0.f));
-        // Walk the visiting order backwards: every qualifying child but the
-        // first is pushed (so they pop in visiting order after the first
-        // child's subtree), the first becomes the current entry.  At most 4
-        // pass (one octant per crossing of each of the three midplanes).
-        StackEntry pend;
+    if (!open) return;
+    const uint4 nd = __ldg(nodes + node);
+    lp = nd.z;
+    lend = nd.z + nd.w;
+    if (!nd.y) return;
+    const float3 half = f3(__fdiv_rn(__fsub_rn(hi.x, lo.x), 2.0f), __fdiv_rn(__fsub_rn(hi.y, lo.y), 2.0f),
+                           __fdiv_rn(__fsub_rn(hi.z, lo.z), 2.0f));
+    // Per axis the children's bounds take two values each: the near half
+    // spans [lo, lo + half], the far half [lo + half, lo + half + half] --
+    // the same rounded sums as the reference's child ranges.
+    const float3 mid = f3(__fadd_rn(lo.x, half.x), __fadd_rn(lo.y, half.y), __fadd_rn(lo.z, half.z));
+    const float3 far = f3(__fadd_rn(mid.x, half.x), __fadd_rn(mid.y, half.y), __fadd_rn(mid.z, half.z));
+    const float3 near_lo = f3(__fadd_rn(lo.x, 0.f), __fadd_rn(lo.y, 0.f), __fadd_rn(lo.z, 0.f));
+    // Walk the visiting order backwards: every qualifying child but the
+    // first is pushed (so they pop in visiting order after the first child's
+    // subtree), the first becomes the current entry.  At most 4 pass (one
+    // octant per crossing of each of the three midplanes).
+    StackEntry pend;
 #pragma unroll
-        for (int i = 7; i >= 0; i--) {
-          const uint32_t cb = (i == 3) ? 4u : (i == 4) ? 3u : uint32_t(i);
-          const uint32_t slot = cb ^ octant;
-          if (!((nd.y >> slot) & 1u)) continue;
-          const float3 clo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y,
-                                (cb & 1) ? mid.z : near_lo.z);
-          const float3 chi = f3((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z);
-          if (!gate_open(cb, t0, t1, clo, chi) || !slab_open(t0, t1, clo, chi)) continue;
-          const uint32_t c = nd.x + __popc(nd.y & ((1u << slot) - 1u));
-          if (have) {
-            if (sp < STACK) stk[sp++] = pend;
-            else cnt.overflow = 1;
-          }
-          pend.lo = make_float4(clo.x, clo.y, clo.z, __uint_as_float(c));
-          pend.hi = make_float4(chi.x, chi.y, chi.z, __uint_as_float(cb | kGateFlag));
-          have = true;
-        }
-        if (have) {
-          node = __float_as_uint(pend.lo.w);
-          gate = __float_as_uint(pend.hi.w);
-          lo = xyz(pend.lo);
-          hi = xyz(pend.hi);
-        }
+    for (int i = 7; i >= 0; i--) {
+      const uint32_t cb = (i == 3) ? 4u : (i == 4) ? 3u : uint32_t(i);
+      const uint32_t slot = cb ^ octant;
+      if (!((nd.y >> slot) & 1u)) continue;
+      const float3 clo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y,
+                            (cb & 1) ? mid.z : near_lo.z);
+      const float3 chi = f3((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z);
+      if (!gate_open(cb, t0, t1, clo, chi) || !slab_open(t0, t1, clo, chi)) continue;
+      const uint32_t c = nd.x + __popc(nd.y & ((1u << slot) - 1u));
+      if (have) {
+        if (sp < STACK) stk[sp++] = pend;
+        else cnt.overflow = 1;
       }
+      pend.lo = make_float4(clo.x, clo.y, clo.z, __uint_as_float(c));
+      pend.hi = make_float4(chi.x, chi.y, chi.z, __uint_as_float(cb | kGateFlag));
+      have = true;
     }
-    return lp >= lend && !have && sp == 0;
+    if (have) {
+      node = __float_as_uint(pend.lo.w);
+      gate = __float_as_uint(pend.hi.w);
+      lo = xyz(pend.lo);
+      hi = xyz(pend.hi);
+    }
   }
 };
+
+// Position of the K-th (1-based) set bit of MASK; MASK has at least K bits set.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t mask, uint32_t k) {
+  uint32_t p = 0;
+#pragma unroll
+  for (uint32_t w = 16; w >= 1; w >>= 1) {
+    const uint32_t c = __popc((mask >> p) & ((1u << w) - 1u));   // set bits in [p, p + w)
+    if (c < k) {
+      k -= c;
+      p += w;
+    }
+  }
+  return p;
+}
+
+// One warp-cooperative round of list tests.  Every lane with a list pending
+// (WANT) owns the next entries of its list; the warp's pending entries, in
+// lane order and list order, are dealt to its 32 lanes (at most 32 per round),
+// each lane tests one entry against its owner's ray, and each owner takes the
+// result of its own entries:
+//  * closest queries: the smallest hit t, the earliest entry among equal t.
+//    This is what the sequential test with a shrinking t1 keeps -- an entry
+//    hits when its t (which does not depend on t1) is below t1 -- so the
+//    result equals the reference's one-by-one loop;
+//  * any-hit queries (ANY): the earliest entry that hits, where the
+//    reference's loop stops.
+// Test counts are the reference's (all entries, or up to the stopping one).
+// All 32 lanes must call it together.  Returns true for an any-hit lane whose
+// search is over.
+template <int STACK>
+__device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool any, TraceCounters &cnt) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t c = want ? tr.lend - tr.lp : 0u;
+  c = c < 32u ? c : 32u;
+  uint32_t incl = c;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t v = __shfl_up_sync(kFull, incl, off);
+    if (lane >= uint32_t(off)) incl += v;
+  }
+  const uint32_t excl = incl - c;
+  const bool owner = c > 0u && excl < 32u;
+  const uint32_t owners = __ballot_sync(kFull, owner);
+  if (owners == 0u) return false;
+  const uint32_t starts = __reduce_or_sync(kFull, owner ? (1u << excl) : 0u);
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  const bool item = lane < total;
+  const uint32_t upto = lane == 31u ? kFull : ((2u << lane) - 1u);
+  const uint32_t own = item ? nth_set_bit(owners, uint32_t(__popc(starts & upto))) : lane;
+  // The owner's ray and list.
+  const uint32_t o_excl = __shfl_sync(kFull, excl, own);
+  const uint32_t o_lp = __shfl_sync(kFull, tr.lp, own);
+  const unsigned long long o_plist =
+      __shfl_sync(kFull, (unsigned long long)reinterpret_cast<uintptr_t>(tr.plist), own);
+  const unsigned long long o_prims =
+      __shfl_sync(kFull, (unsigned long long)reinterpret_cast<uintptr_t>(tr.prims), own);
+  const float3 ro = f3(__shfl_sync(kFull, tr.o.x, own), __shfl_sync(kFull, tr.o.y, own),
+                       __shfl_sync(kFull, tr.o.z, own));
+  const float3 rd = f3(__shfl_sync(kFull, tr.d.x, own), __shfl_sync(kFull, tr.d.y, own),
+                       __shfl_sync(kFull, tr.d.z, own));
+  const float rt0 = __shfl_sync(kFull, tr.t0, own);
+  const float rt1 = __shfl_sync(kFull, tr.t1, own);
+  const bool o_any = (__ballot_sync(kFull, any) >> own) & 1u;
+  uint32_t pid = PREF_END;
+  bool hit = false;
+  float th = rt1;
+  if (item) {
+    pid = __ldg(reinterpret_cast<const uint32_t *>(o_plist) + o_lp + (lane - o_excl));
+    const float4 *p = reinterpret_cast<const float4 *>(o_prims) + 3 * size_t(pid);
+    const PrimRec r{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+    hit = test_prim(r, ro, rd, rt0, th);
+  }
+  // Reduce over each owner's entries (positive t: its bits order like the value).
+  const unsigned grp = __match_any_sync(kFull, item ? own : 32u + lane);
+  const uint32_t tb = hit ? __float_as_uint(th) : kFull;
+  const uint32_t tmin = __reduce_min_sync(grp, tb);
+  const uint32_t best = __reduce_min_sync(grp, (hit && (o_any || tb == tmin)) ? lane : kFull);
+  // Each owner reads the result at its first entry's lane.
+  const uint32_t b = __shfl_sync(kFull, best, owner ? excl : lane);
+  const uint32_t src = b < 32u ? b : lane;
+  const uint32_t b_pid = __shfl_sync(kFull, pid, src);
+  const float b_t = __shfl_sync(kFull, th, src);
+  if (!owner) return false;
+  const uint32_t used = c < 32u - excl ? c : 32u - excl;
+  if (b < 32u) {
+    tr.hit_ref = b_pid;
+    if (any) {
+      cnt.tests += b - excl + 1u;
+      tr.lp = tr.lend;
+      return true;
+    }
+    tr.t1 = b_t;
+  }
+  cnt.tests += used;
+  tr.lp += used;
+  return false;
+}
 
 // Warp-cooperative ray dispenser for the persistent trace kernels: lanes
 // whose ray is finished take the next index from a warp-local range of CHUNK
@@ -388,6 +456,38 @@ struct RayDispenser {
     return got;
   }
 };
+
+// The persistent trace loop shared by the trace kernels.  Lanes take rays
+// from DISPENSER (n rays) through a RayDispenser; START(i, tr, any) begins ray
+// i (calls tr.init and sets ANY for an any-hit query); DONE(i, tr, any)
+// stores its result.  Each iteration every live lane without a list pending
+// visits one octree entry, then the warp tests one round of pending list
+// entries together.  All 32 lanes of every warp must run it.
+template <int STACK, class Start, class Done>
+__device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, TraceCounters &cnt, Start start,
+                                           Done done) {
+  Traversal<STACK> tr;
+  RayDispenser disp;
+  uint32_t ray = RayDispenser::kIdle;
+  bool any = false;
+  for (;;) {
+    bool all_idle;
+    const uint32_t got =
+        disp.fetch(dispenser, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
+    if (all_idle) break;
+    if (got != RayDispenser::kIdle) {
+      ray = got;
+      start(ray, tr, any);
+    }
+    const bool busy = ray != RayDispenser::kIdle;
+    if (busy && tr.lp >= tr.lend && !tr.finished()) tr.node_step(cnt);
+    const bool stop = list_round(tr, busy && tr.lp < tr.lend, any, cnt);
+    if (busy && (stop || tr.finished())) {
+      done(ray, tr, any);
+      ray = RayDispenser::kIdle;
+    }
+  }
+}
 
 // Global primitive id of a packed reference: triangles, then spheres, then
 // tripars.

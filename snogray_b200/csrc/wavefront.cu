@@ -113,27 +113,18 @@ __global__ void __launch_bounds__(128, 6) k_trace_closest(DevScene s, RayQ q, ui
     counters[5] = 0;          // shadow kernel's dispenser
     stats[0] += n;
   }
-  unsigned long long nodes = 0, tests = 0;
-  Traversal<STACK> tr;
-  RayDispenser disp;
-  uint32_t ray = RayDispenser::kIdle;
   TraceCounters c{0, 0, 0};
-  for (;;) {
-    bool all_idle;
-    const uint32_t got = disp.fetch(counters + 4, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle,
-                                    &all_idle);
-    if (all_idle) break;
-    if (got != RayDispenser::kIdle) {
-      ray = got;
-      const float4 o = q.o[ray], d = q.d[ray];
-      tr.init(s, xyz(o), xyz(d), o.w, d.w);
-    }
-    if (ray == RayDispenser::kIdle) continue;
-    if (!tr.template step<false>(s, c)) continue;
-    hit_ref[ray] = tr.hit_ref;
-    hit_t[ray] = tr.t1;
-    ray = RayDispenser::kIdle;
-  }
+  trace_loop<STACK>(
+      counters + 4, n, c,
+      [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
+        const float4 o = q.o[ray], d = q.d[ray];
+        tr.init(s, xyz(o), xyz(d), o.w, d.w);
+        any = false;
+      },
+      [&](uint32_t ray, Traversal<STACK> &tr, bool) {
+        hit_ref[ray] = tr.hit_ref;
+        hit_t[ray] = tr.t1;
+      });
   if (c.overflow) atomicOr(counters + 3, 1u);
   if (prof) warp_count(stats + 2, c.nodes, c.tests);
 }
@@ -145,31 +136,22 @@ __global__ void __launch_bounds__(128, 6) k_trace_shadow(DevScene s, ShadowQ q, 
                                                       unsigned long long *stats, bool prof) {
   const uint32_t n = counters[2];
   if (blockIdx.x == 0 && threadIdx.x == 0) stats[1] += n;
-  Traversal<STACK> tr;
-  RayDispenser disp;
-  uint32_t ray = RayDispenser::kIdle;
   TraceCounters c{0, 0, 0};
-  for (;;) {
-    bool all_idle;
-    const uint32_t got = disp.fetch(counters + 5, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle,
-                                    &all_idle);
-    if (all_idle) break;
-    if (got != RayDispenser::kIdle) {
-      ray = got;
-      const float4 o = q.o[ray], d = q.d[ray];
-      tr.init(s, xyz(o), xyz(d), o.w, d.w);
-    }
-    if (ray == RayDispenser::kIdle) continue;
-    if (!tr.template step<true>(s, c)) continue;
-    if (tr.hit_ref == PREF_END) {
-      float4 cc = q.c[ray];
-      float4 *r = rad + __float_as_uint(cc.w);
-      atomicAdd(&r->x, cc.x);
-      atomicAdd(&r->y, cc.y);
-      atomicAdd(&r->z, cc.z);
-    }
-    ray = RayDispenser::kIdle;
-  }
+  trace_loop<STACK>(
+      counters + 5, n, c,
+      [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
+        const float4 o = q.o[ray], d = q.d[ray];
+        tr.init(s, xyz(o), xyz(d), o.w, d.w);
+        any = true;
+      },
+      [&](uint32_t ray, Traversal<STACK> &tr, bool) {
+        if (tr.hit_ref != PREF_END) return;
+        const float4 cc = q.c[ray];
+        float4 *r = rad + __float_as_uint(cc.w);
+        atomicAdd(&r->x, cc.x);
+        atomicAdd(&r->y, cc.y);
+        atomicAdd(&r->z, cc.z);
+      });
   if (c.overflow) atomicOr(counters + 3, 1u);
   if (prof) warp_count(stats + 4, c.nodes, c.tests);
 }

@@ -51,7 +51,7 @@ def _compile(src, force):
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
         return obj, ""
     if src.endswith(".cu"):
-        cmd = [NVCC, *NVCCFLAGS, "-c", src, "-o", obj]
+        cmd = [NVCC, *NVCCFLAGS, *os.environ.get("SNOG_NVCC_FLAGS", "").split(), "-c", src, "-o", obj]
     else:
         cmd = ["g++", *CXXFLAGS, "-c", src, "-o", obj]
     out = subprocess.run(cmd, capture_output=True, text=True)

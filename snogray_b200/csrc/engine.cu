@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256) k_e_regen(EngineCtl *ctl, const WorkItem 
 }
 
 template <int STACK>
-__global__ void __launch_bounds__(128, 6) k_e_closest(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
+__global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_closest(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
                                                       const DevScene *scenes, EQ q, uint32_t *hit_ref,
                                                       float *hit_t) {
   const uint32_t n = ctl->qcount[cur];
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128, 6) k_e_closest(EngineCtl *ctl, uint32_t c
 }
 
 template <int STACK>
-__global__ void __launch_bounds__(128, 6) k_e_shadow(EngineCtl *ctl, const DevScene *scenes, ESQ q) {
+__global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_shadow(EngineCtl *ctl, const DevScene *scenes, ESQ q) {
   const uint32_t n = ctl->scount;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_shadow += n;
   TraceCounters c{0, 0, 0};
@@ -370,12 +370,12 @@ void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uin
   k_e_plan<<<1, 1, 0, st>>>(ctl, ring, R, N, cur);
   k_e_regen<<<sms * 8, 256, 0, st>>>(ctl, ring, R, jobs, qc);
   if (ev) cudaEventRecord(ev[1], st);
-  k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, 128), 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
+  k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
                                                                                hit_t);
   if (ev) cudaEventRecord(ev[2], st);
   k_e_shade<<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done);
   if (ev) cudaEventRecord(ev[3], st);
-  k_e_shadow<STACK><<<resident_grid(k_e_shadow<STACK>, 128), 128, 0, st>>>(ctl, scenes, sq);
+  k_e_shadow<STACK><<<resident_grid(k_e_shadow<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, scenes, sq);
   if (ev) cudaEventRecord(ev[4], st);
 }
 

@@ -12,7 +12,7 @@
 namespace snog {
 
 template <int STACK>
-__global__ void __launch_bounds__(128) k_trace_batch(DevScene s, const float *__restrict__ rays,
+__global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_batch(DevScene s, const float *__restrict__ rays,
                                                      uint32_t n, uint32_t n_closest,
                                                      int32_t *__restrict__ prim, float *__restrict__ tout,
                                                      float *__restrict__ nrm,
@@ -94,7 +94,7 @@ cudaError_t launch_trace_batch(const DevScene &s, const float *rays, uint32_t n,
                                int32_t *prim, float *t, float *nrm, unsigned long long *counters,
                                uint32_t *err, uint32_t *fetch, cudaStream_t st, int *launches) {
   if (n == 0) return cudaSuccess;
-  const int threads = 128;
+  const int threads = kTraceBlock;
   const uint32_t want = (n + threads - 1) / threads;
   auto grid = [&](uint32_t resident) { return want < resident ? want : resident; };
   switch (stack_class_for_depth(s.max_depth)) {

@@ -173,6 +173,13 @@ struct StackEntry {
   float4 lo, hi;
 };
 
+// Threads per block of every trace kernel.
+constexpr int kTraceBlock = 128;
+// Blocks per SM the trace kernels are compiled for (register cap 64).
+#ifndef SNOG_TRACE_MINBLOCKS
+#define SNOG_TRACE_MINBLOCKS 8
+#endif
+
 constexpr uint32_t kGateFlag = 8u;   // entry carries a parent gate
 
 __device__ __forceinline__ bool slab_open(float t0, float t1, float3 lo, float3 hi) {
@@ -460,8 +467,9 @@ struct RayDispenser {
 // The persistent trace loop shared by the trace kernels.  Lanes take rays
 // from DISPENSER (n rays) through a RayDispenser; START(i, tr, any) begins ray
 // i (calls tr.init and sets ANY for an any-hit query); DONE(i, tr, any)
-// stores its result.  Each iteration every live lane without a list pending
-// visits one octree entry, then the warp tests one round of pending list
+// stores its result.  Each iteration, unless the warp already has a full
+// round of list entries pending, every live lane without a list pending
+// visits one octree entry; then the warp tests one round of pending list
 // entries together.  All 32 lanes of every warp must run it.
 template <int STACK, class Start, class Done>
 __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, TraceCounters &cnt, Start start,
@@ -480,7 +488,11 @@ __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, Trac
       start(ray, tr, any);
     }
     const bool busy = ray != RayDispenser::kIdle;
-    if (busy && tr.lp >= tr.lend && !tr.finished()) tr.node_step(cnt);
+    // Visit nodes only while the warp's pending list entries would not fill
+    // a round: list rounds run full, node steps run with more lanes at once.
+    const uint32_t pend = (busy && tr.lp < tr.lend) ? tr.lend - tr.lp : 0u;
+    const uint32_t pending = __reduce_add_sync(0xffffffffu, pend < 32u ? pend : 32u);
+    if (pending < 32u && busy && tr.lp >= tr.lend && !tr.finished()) tr.node_step(cnt);
     const bool stop = list_round(tr, busy && tr.lp < tr.lend, any, cnt);
     if (busy && (stop || tr.finished())) {
       done(ray, tr, any);

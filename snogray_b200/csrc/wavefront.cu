@@ -103,7 +103,7 @@ __device__ __forceinline__ void warp_count(unsigned long long *p, unsigned long 
 // RayDispenser (counters[4]) and interleave one octree entry per ray per
 // iteration, so finished lanes are refilled instead of idling.
 template <int STACK>
-__global__ void __launch_bounds__(128, 6) k_trace_closest(DevScene s, RayQ q, uint32_t *counters, uint32_t cur,
+__global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_closest(DevScene s, RayQ q, uint32_t *counters, uint32_t cur,
                                                        uint32_t *hit_ref, float *hit_t,
                                                        unsigned long long *stats, bool prof) {
   const uint32_t n = counters[cur];
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128, 6) k_trace_closest(DevScene s, RayQ q, ui
 // Persistent any-hit kernel for the shadow queue (dispenser counters[5]);
 // an unoccluded ray adds its contribution to its path's radiance.
 template <int STACK>
-__global__ void __launch_bounds__(128, 6) k_trace_shadow(DevScene s, ShadowQ q, uint32_t *counters, float4 *rad,
+__global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_shadow(DevScene s, ShadowQ q, uint32_t *counters, float4 *rad,
                                                       unsigned long long *stats, bool prof) {
   const uint32_t n = counters[2];
   if (blockIdx.x == 0 && threadIdx.x == 0) stats[1] += n;
@@ -452,11 +452,11 @@ void launch_bounce(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, uint
   PathPtrs P{wb.thr, wb.rad, wb.pstate, wb.jit};
   const bool pf = prof != nullptr;
   if (pf) prof->begin(st, RenderProfile::CLOSEST);
-  k_trace_closest<STACK><<<resident_grid(k_trace_closest<STACK>, 128), 128, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
+  k_trace_closest<STACK><<<resident_grid(k_trace_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
   if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADE);
   k_shade<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, P, qout, sq);
   if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADOW);
-  k_trace_shadow<STACK><<<resident_grid(k_trace_shadow<STACK>, 128), 128, 0, st>>>(s, sq, wb.counters, wb.rad, wb.stats, pf);
+  k_trace_shadow<STACK><<<resident_grid(k_trace_shadow<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(s, sq, wb.counters, wb.rad, wb.stats, pf);
   if (pf) prof->end(st);
 }
 

@@ -53,28 +53,47 @@ void OctreeBuilder::push_ref(uint32_t node, uint32_t ref) {
   head_[node] = slot;
 }
 
+void root_start(const Box3 &b, float origin[3], float &size) {
+  for (int k = 0; k < 3; k++) origin[k] = b.lo[k];
+  size = box_max_size(b);
+}
+
+bool root_fits(const float origin[3], float size, const Box3 &b) {
+  return origin[0] <= b.lo[0] && origin[1] <= b.lo[1] && origin[2] <= b.lo[2] &&
+         (origin[0] + size) >= b.hi[0] && (origin[1] + size) >= b.hi[1] && (origin[2] + size) >= b.hi[2];
+}
+
+// On each axis the cube grows to the side where B sticks out further (ties
+// grow downwards); the old root keeps its position as one octant.
+uint32_t root_grow(const Box3 &b, float origin[3], float &size) {
+  uint32_t octant = 0;
+  for (int a = 0; a < 3; a++) {
+    float lo_grow = origin[a] - b.lo[a];
+    float hi_grow = b.hi[a] - (origin[a] + size);
+    bool grow_up = hi_grow > lo_grow;
+    // Octant bit for axis a: x = 4, y = 2, z = 1 (space/octree-node.h:35-39).
+    if (!grow_up) {
+      octant |= 4u >> a;
+      origin[a] -= size;
+    }
+  }
+  size *= 2;
+  return octant;
+}
+
 void OctreeBuilder::add(uint32_t ref, const Box3 &b) {
   if (head_.empty()) {
     new_node();
-    for (int k = 0; k < 3; k++) origin_[k] = b.lo[k];
-    size_ = box_max_size(b);
+    root_start(b, origin_, size_);
     push_ref(0, ref);
     return;
   }
-  for (;;) {
-    bool fits = origin_[0] <= b.lo[0] && origin_[1] <= b.lo[1] && origin_[2] <= b.lo[2] &&
-                (origin_[0] + size_) >= b.hi[0] && (origin_[1] + size_) >= b.hi[1] &&
-                (origin_[2] + size_) >= b.hi[2];
-    if (fits) break;
-    grow_towards(b);
-  }
+  while (!root_fits(origin_, size_, b)) grow_towards(b);
   insert(ref, b, 0, origin_[0], origin_[1], origin_[2], size_);
 }
 
-// Double the root cube towards B: on each axis the cube grows to the side
-// where B sticks out further (ties grow downwards), and the old root becomes
-// the octant that keeps its old position.  Node 0 stays the root, so the old
-// root's record moves to a fresh slot.
+// Double the root cube towards B.  Node 0 stays the root, so the old root's
+// record moves to a fresh slot, which becomes the new root's child.
 void OctreeBuilder::grow_towards(const Box3 &b) {
   uint32_t moved = new_node();
   for (int k = 0; k < 8; k++) {
@@ -83,20 +102,7 @@ void OctreeBuilder::grow_towards(const Box3 &b) {
   }
   head_[moved] = head_[0];
   head_[0] = 0;
-
-  uint32_t octant = 0;
-  for (int a = 0; a < 3; a++) {
-    float lo_grow = origin_[a] - b.lo[a];
-    float hi_grow = b.hi[a] - (origin_[a] + size_);
-    bool grow_up = hi_grow > lo_grow;
-    // Octant bit for axis a: x = 4, y = 2, z = 1 (space/octree-node.h:35-39).
-    if (!grow_up) {
-      octant |= 4u >> a;
-      origin_[a] -= size_;
-    }
-  }
-  kids_[octant] = moved;
-  size_ *= 2;
+  kids_[root_grow(b, origin_, size_)] = moved;
 }
 
 void OctreeBuilder::insert(uint32_t ref, const Box3 &b, uint32_t node, float x, float y, float z,

@@ -43,6 +43,16 @@ struct OctreeArrays {
   uint64_t n_list_surfaces = 0;
 };
 
+// Root cube of the tree being built: the first surface fixes it at its bbox
+// minimum with side bbox.max_size(); a later surface outside it doubles it
+// towards the surface, the old root becoming one octant of the new one
+// (space/octree-builder.cc:173-247).  Shared by the host and device builders
+// so both grow the root with the same float operations.
+void root_start(const Box3 &box, float origin[3], float &size);
+bool root_fits(const float origin[3], float size, const Box3 &box);
+// Doubles the cube towards BOX; returns the octant the old root becomes.
+uint32_t root_grow(const Box3 &box, float origin[3], float &size);
+
 class OctreeBuilder {
  public:
   // Insert one surface with reference REF (stored verbatim in the lists)

@@ -11,8 +11,15 @@
 
 namespace snog {
 
+// The ray-batch kernel carries per-query counters and the normal output on
+// top of the walk; at 7 blocks per SM (72 registers) it spills a few bytes
+// instead of about a hundred at 8.
+#ifndef SNOG_TRACE_BATCH_MINBLOCKS
+#define SNOG_TRACE_BATCH_MINBLOCKS 7
+#endif
+
 template <int STACK>
-__global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_batch(DevScene s, const float *__restrict__ rays,
+__global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_BATCH_MINBLOCKS) k_trace_batch(DevScene s, const float *__restrict__ rays,
                                                      uint32_t n, uint32_t n_closest,
                                                      int32_t *__restrict__ prim, float *__restrict__ tout,
                                                      float *__restrict__ nrm,

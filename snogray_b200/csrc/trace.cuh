@@ -62,7 +62,7 @@ __device__ __forceinline__ bool tripar_hit(float3 corner, float3 e1, float3 e2, 
   float3 pvec = xcross(d, e2);
   float det = xdot(e1, pvec);
   if (det > -kEps && det < kEps) return false;
-  float inv_det = __fdiv_rn(1.0f, det);
+  float inv_det = __frcp_rn(det);   // = 1.0f / det, correctly rounded
   float3 tvec = xsub(o, corner);
   u = __fmul_rn(xdot(tvec, pvec), inv_det);
   if (u < 0.f || u > 1.f) return false;
@@ -180,6 +180,25 @@ constexpr int kTraceBlock = 128;
 #define SNOG_TRACE_MINBLOCKS 8
 #endif
 
+// The newest kRing entries of each thread's traversal stack live in shared
+// memory, as a ring; older entries spill to the thread's local-memory array.
+// Lanes of a warp sit at different stack depths, so a local-memory stack is
+// read and written uncoalesced and every push is written through to L2; the
+// ring keeps the pushes and pops of a walk on chip (kRing * 32 bytes per
+// thread, 16 KB per 128-thread block at kRing = 4).
+#ifndef SNOG_RING
+#define SNOG_RING 4
+#endif
+constexpr uint32_t kRing = SNOG_RING;
+
+// This thread's first ring slot.  Entry position e of thread t is float4
+// 2 * e * kTraceBlock + t (lo) and (2 * e + 1) * kTraceBlock + t (hi): a warp
+// touching one position reads 512 contiguous bytes.
+__device__ __forceinline__ float4 *ring_slots() {
+  __shared__ float4 ring[2 * kRing * kTraceBlock];
+  return ring + threadIdx.x;
+}
+
 constexpr uint32_t kGateFlag = 8u;   // entry carries a parent gate
 
 __device__ __forceinline__ bool slab_open(float t0, float t1, float3 lo, float3 hi) {
@@ -200,22 +219,27 @@ __device__ __forceinline__ bool gate_open(uint32_t cb, float t0, float t1, float
   return gx && gy && gz;
 }
 
+// Octant bits (x = 4, y = 2, z = 1) of the I-th child in the reference's
+// visiting order 0,1,2,4,3,5,6,7 (before the xor with the ray's octant).
+__device__ __forceinline__ uint32_t visit_bits(uint32_t i) { return i == 3u ? 4u : i == 4u ? 3u : i; }
+
 // A resumable octree walk for one ray.  init() sets up the root's slab
 // bounds (space/octree.cc:119-135); node_step() processes one octree entry --
 // the child entered last, else the top of the stack -- as one call of the
 // reference's recursive function does: parent gate, slab cull, then the
 // node's surface list (left pending in [lp, lend) for list_round) and the
 // children.  Kernels interleave the steps of many rays per warp and refill
-// lanes whose ray has finished.  STACK entries must cover 3 * depth + 2
-// (chosen by the host from the tree depth); if they do not, cnt.overflow is
-// set and the result must be discarded.
+// lanes whose ray has finished.  STACK + kRing entries must cover
+// 3 * depth + 2 (the host picks STACK from the tree depth); if they do not,
+// cnt.overflow is set and the result must be discarded.
 template <int STACK>
 struct Traversal {
   float3 o, d, lo, hi;
   float t0, t1;
   uint32_t node, gate, octant, hit_ref;
   uint32_t lp, lend;         // surface list still to test: plist[lp, lend)
-  int sp;
+  uint32_t ring;             // shared-memory ring: oldest position | count << 4 (0 when empty)
+  int sp;                    // entries spilled to stk[0, sp)
   bool have;                 // a current entry (node/gate/lo/hi) is set
   const uint4 *nodes;        // the ray's scene
   const uint32_t *plist;
@@ -229,6 +253,7 @@ struct Traversal {
     t1 = t1_;
     hit_ref = PREF_END;
     sp = 0;
+    ring = 0;
     node = 0;
     gate = 0;
     lp = lend = 0;
@@ -236,17 +261,19 @@ struct Traversal {
     nodes = s.nodes;
     plist = s.plist;
     prims = s.prims;
-    float inv = (d.x == 0.f) ? 1e9f : __fdiv_rn(1.0f, d.x);
+    // 1 / d rounded once, as the reference's division (__frcp_rn is the
+    // correctly rounded reciprocal, the same value as 1.0f / d).
+    float inv = (d.x == 0.f) ? 1e9f : __frcp_rn(d.x);
     float a = __fmul_rn(__fsub_rn(s.origin[0], o.x), inv);
     float b = __fmul_rn(__fadd_rn(__fsub_rn(s.origin[0], o.x), s.size), inv);
     if (a > b) { float tmp = a; a = b; b = tmp; }
     lo.x = a; hi.x = b;
-    inv = (d.y == 0.f) ? 1e9f : __fdiv_rn(1.0f, d.y);
+    inv = (d.y == 0.f) ? 1e9f : __frcp_rn(d.y);
     a = __fmul_rn(__fsub_rn(s.origin[1], o.y), inv);
     b = __fmul_rn(__fadd_rn(__fsub_rn(s.origin[1], o.y), s.size), inv);
     if (a > b) { float tmp = a; a = b; b = tmp; }
     lo.y = a; hi.y = b;
-    inv = (d.z == 0.f) ? 1e9f : __fdiv_rn(1.0f, d.z);
+    inv = (d.z == 0.f) ? 1e9f : __frcp_rn(d.z);
     a = __fmul_rn(__fsub_rn(s.origin[2], o.z), inv);
     b = __fmul_rn(__fadd_rn(__fsub_rn(s.origin[2], o.z), s.size), inv);
     if (a > b) { float tmp = a; a = b; b = tmp; }
@@ -255,7 +282,56 @@ struct Traversal {
   }
 
   // The walk is over: no list pending, no current entry, empty stack.
-  __device__ __forceinline__ bool finished() const { return lp >= lend && !have && sp == 0; }
+  __device__ __forceinline__ bool finished() const { return lp >= lend && !have && sp == 0 && (ring >> 4) == 0u; }
+
+  // Push an entry: into the ring, first moving the ring's oldest entry to
+  // local memory when the ring is full.
+  __device__ __forceinline__ void push(float4 elo, float4 ehi, TraceCounters &cnt) {
+    float4 *r = ring_slots();
+    uint32_t base = ring & 15u, n = ring >> 4;
+    if (n == kRing) {
+      if (sp < STACK) {
+        stk[sp].lo = r[2 * base * kTraceBlock];
+        stk[sp].hi = r[(2 * base + 1) * kTraceBlock];
+        sp++;
+      } else {
+        cnt.overflow = 1;
+      }
+      base = base + 1u == kRing ? 0u : base + 1u;
+      n--;
+    }
+    uint32_t pos = base + n;
+    pos = pos >= kRing ? pos - kRing : pos;
+    r[2 * pos * kTraceBlock] = elo;
+    r[(2 * pos + 1) * kTraceBlock] = ehi;
+    ring = base | ((n + 1u) << 4);
+  }
+
+  // Pop the newest entry into the current one.  Returns false (and leaves
+  // the walk unchanged) if nothing is stacked.
+  __device__ __forceinline__ bool pop() {
+    float4 elo, ehi;
+    const uint32_t base = ring & 15u, n = ring >> 4;
+    if (n) {
+      const float4 *r = ring_slots();
+      uint32_t pos = base + n - 1u;
+      pos = pos >= kRing ? pos - kRing : pos;
+      elo = r[2 * pos * kTraceBlock];
+      ehi = r[(2 * pos + 1) * kTraceBlock];
+      ring = n > 1u ? (base | ((n - 1u) << 4)) : 0u;   // an emptied ring restarts at position 0
+    } else if (sp > 0) {
+      --sp;
+      elo = stk[sp].lo;
+      ehi = stk[sp].hi;
+    } else {
+      return false;
+    }
+    node = __float_as_uint(elo.w);
+    gate = __float_as_uint(ehi.w);
+    lo = xyz(elo);
+    hi = xyz(ehi);
+    return true;
+  }
 
   // One octree entry (call only with no list pending and !finished()).
   //
@@ -267,13 +343,7 @@ struct Traversal {
   // every entry's gate and cull are evaluated again when it is entered -- so
   // the tests and their order are the reference's.
   __device__ __forceinline__ void node_step(TraceCounters &cnt) {
-    if (!have) {
-      --sp;
-      node = __float_as_uint(stk[sp].lo.w);
-      gate = __float_as_uint(stk[sp].hi.w);
-      lo = xyz(stk[sp].lo);
-      hi = xyz(stk[sp].hi);
-    }
+    if (!have && !pop()) return;
     have = false;
     bool open = true;
     if (gate & kGateFlag) open = gate_open(gate & 7u, t0, t1, lo, hi);
@@ -286,43 +356,52 @@ struct Traversal {
     lp = nd.z;
     lend = nd.z + nd.w;
     if (!nd.y) return;
-    const float3 half = f3(__fdiv_rn(__fsub_rn(hi.x, lo.x), 2.0f), __fdiv_rn(__fsub_rn(hi.y, lo.y), 2.0f),
-                           __fdiv_rn(__fsub_rn(hi.z, lo.z), 2.0f));
+    // (hi - lo) / 2: halving rounds exactly like the reference's division by 2.
+    const float3 half = f3(__fmul_rn(__fsub_rn(hi.x, lo.x), 0.5f), __fmul_rn(__fsub_rn(hi.y, lo.y), 0.5f),
+                           __fmul_rn(__fsub_rn(hi.z, lo.z), 0.5f));
     // Per axis the children's bounds take two values each: the near half
     // spans [lo, lo + half], the far half [lo + half, lo + half + half] --
     // the same rounded sums as the reference's child ranges.
     const float3 mid = f3(__fadd_rn(lo.x, half.x), __fadd_rn(lo.y, half.y), __fadd_rn(lo.z, half.z));
     const float3 far = f3(__fadd_rn(mid.x, half.x), __fadd_rn(mid.y, half.y), __fadd_rn(mid.z, half.z));
     const float3 near_lo = f3(__fadd_rn(lo.x, 0.f), __fadd_rn(lo.y, 0.f), __fadd_rn(lo.z, 0.f));
-    // Walk the visiting order backwards: every qualifying child but the
-    // first is pushed (so they pop in visiting order after the first child's
-    // subtree), the first becomes the current entry.  At most 4 pass (one
-    // octant per crossing of each of the three midplanes).
-    StackEntry pend;
+    // Which children pass gate and cull, by visiting position (bit i).  At
+    // most 4 pass: one octant per crossing of each of the three midplanes.
+    uint32_t vm = 0;
 #pragma unroll
-    for (int i = 7; i >= 0; i--) {
-      const uint32_t cb = (i == 3) ? 4u : (i == 4) ? 3u : uint32_t(i);
+    for (uint32_t i = 0; i < 8; i++) {
+      const uint32_t cb = visit_bits(i);
       const uint32_t slot = cb ^ octant;
-      if (!((nd.y >> slot) & 1u)) continue;
       const float3 clo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y,
                             (cb & 1) ? mid.z : near_lo.z);
       const float3 chi = f3((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z);
-      if (!gate_open(cb, t0, t1, clo, chi) || !slab_open(t0, t1, clo, chi)) continue;
+      const bool ok = ((nd.y >> slot) & 1u) & gate_open(cb, t0, t1, clo, chi) & slab_open(t0, t1, clo, chi);
+      vm |= ok ? (1u << i) : 0u;
+    }
+    if (!vm) return;
+    // Every qualifying child but the first is pushed, in reverse visiting
+    // order, so they pop in visiting order after the first child's subtree;
+    // the first becomes the current entry.
+    for (uint32_t m = vm & (vm - 1u); m;) {
+      const uint32_t i = 31u - __clz(m);
+      m &= ~(1u << i);
+      const uint32_t cb = visit_bits(i);
+      const uint32_t slot = cb ^ octant;
       const uint32_t c = nd.x + __popc(nd.y & ((1u << slot) - 1u));
-      if (have) {
-        if (sp < STACK) stk[sp++] = pend;
-        else cnt.overflow = 1;
-      }
-      pend.lo = make_float4(clo.x, clo.y, clo.z, __uint_as_float(c));
-      pend.hi = make_float4(chi.x, chi.y, chi.z, __uint_as_float(cb | kGateFlag));
-      have = true;
+      push(make_float4((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y, (cb & 1) ? mid.z : near_lo.z,
+                       __uint_as_float(c)),
+           make_float4((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z,
+                       __uint_as_float(cb | kGateFlag)),
+           cnt);
     }
-    if (have) {
-      node = __float_as_uint(pend.lo.w);
-      gate = __float_as_uint(pend.hi.w);
-      lo = xyz(pend.lo);
-      hi = xyz(pend.hi);
-    }
+    const uint32_t i = __ffs(vm) - 1u;
+    const uint32_t cb = visit_bits(i);
+    const uint32_t slot = cb ^ octant;
+    node = nd.x + __popc(nd.y & ((1u << slot) - 1u));
+    gate = cb | kGateFlag;
+    lo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y, (cb & 1) ? mid.z : near_lo.z);
+    hi = f3((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z);
+    have = true;
   }
 };
 

@@ -159,6 +159,17 @@ int snog_init(int device);
  * (light/envmap-light.cc:103-140, geometry/hist-2d-dist.cc:65-120). */
 int snog_scene_create(const SnogSceneDesc *desc, SnogScene **out);
 
+/* Octree builders for snog_scene_create_ex.  Both give the same tree (node
+ * arrays and list order identical to Octree::Builder's); the device builder
+ * replays the root's growth on the host and places the surfaces in parallel
+ * (octree_gpu.cu).  AUTO, snog_scene_create's choice, uses the device for
+ * scenes of 65536 surfaces or more. */
+enum { SNOG_OCTREE_AUTO = 0, SNOG_OCTREE_HOST = 1, SNOG_OCTREE_DEVICE = 2 };
+
+/* snog_scene_create with the octree builder chosen by OCTREE_MODE; replaces
+ * the same reference path (space/octree-builder.cc:173-650). */
+int snog_scene_create_ex(const SnogSceneDesc *desc, uint32_t octree_mode, SnogScene **out);
+
 /* Build the acceleration structure on the host only, without touching the
  * device (no CUDA context needed): the handle serves snog_scene_info and
  * snog_scene_octree, and is refused by the tracing and rendering calls. */

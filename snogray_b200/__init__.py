@@ -124,6 +124,7 @@ _last_error = _sig("snog_last_error", C.c_char_p)
 _init = _sig("snog_init", C.c_int, C.c_int)
 _scene_create = _sig("snog_scene_create", C.c_int, C.POINTER(SnogSceneDesc), C.POINTER(_P))
 _scene_build_host = _sig("snog_scene_build_host", C.c_int, C.POINTER(SnogSceneDesc), C.POINTER(_P))
+_scene_create_ex = _sig("snog_scene_create_ex", C.c_int, C.POINTER(SnogSceneDesc), C.c_uint32, C.POINTER(_P))
 _scene_destroy = _sig("snog_scene_destroy", C.c_int, _P)
 _scene_info = _sig("snog_scene_info", C.c_int, _P, C.POINTER(SnogSceneInfo))
 _scene_octree = _sig("snog_scene_octree", C.c_int, _P, _P, _P, _P)
@@ -194,7 +195,12 @@ class Scene:
     octree).  Mirrors the reference's GlobalRenderState/Scene pair: built
     once from the surfaces and lights, then rendered or traced."""
 
-    def __init__(self, data: SceneData, device=True):
+    OCTREE_AUTO, OCTREE_HOST, OCTREE_DEVICE = 0, 1, 2
+
+    def __init__(self, data: SceneData, device=True, octree=0):
+        """OCTREE picks the octree builder of a device scene (snog_scene_create_ex):
+        OCTREE_AUTO, OCTREE_HOST or OCTREE_DEVICE; a host-only scene
+        (DEVICE=False) always uses the host builder."""
         self.data = data
         keep = []
 
@@ -225,7 +231,10 @@ class Scene:
             d.env_rgb = _ptr(e)
         d.env_frame[:] = [float(x) for x in np.asarray(data.env_frame, np.float32).reshape(9)]
         h = _P()
-        _check((_scene_create if device else _scene_build_host)(C.byref(d), C.byref(h)))
+        if device:
+            _check(_scene_create_ex(C.byref(d), octree, C.byref(h)))
+        else:
+            _check(_scene_build_host(C.byref(d), C.byref(h)))
         self._h = h
         self.on_device = device
 

@@ -272,10 +272,15 @@ int snog_init(int device) {
 }
 
 int snog_scene_create(const SnogSceneDesc *desc, SnogScene **out) {
+  return snog_scene_create_ex(desc, SNOG_OCTREE_AUTO, out);
+}
+
+int snog_scene_create_ex(const SnogSceneDesc *desc, uint32_t octree_mode, SnogScene **out) {
   return guarded([&] {
     if (!desc || !out) throw Error{SNOG_EINVAL, "null argument"};
+    if (octree_mode > SNOG_OCTREE_DEVICE) throw Error{SNOG_EINVAL, "unknown octree mode"};
     *out = nullptr;
-    SceneImpl *impl = build_scene(*desc);
+    SceneImpl *impl = build_scene(*desc, true, octree_mode);
     *out = new SnogScene{impl};
     return int(SNOG_OK);
   });
@@ -316,8 +321,7 @@ int snog_scene_info(const SnogScene *scene, SnogSceneInfo *info) {
 int snog_scene_octree(const SnogScene *scene, uint32_t *children, uint32_t *heads, int32_t *plist) {
   return guarded([&] {
     if (!scene) throw Error{SNOG_EINVAL, "null argument"};
-    const SceneImpl &S = *scene->impl;
-    const OctreeArrays &o = S.oct;
+    const OctreeArrays &o = host_octree(*scene->impl);
     if (children) std::memcpy(children, o.children.data(), o.children.size() * 4);
     if (heads) std::memcpy(heads, o.heads.data(), o.heads.size() * 4);
     if (plist) {

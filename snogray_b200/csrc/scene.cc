@@ -7,6 +7,8 @@
 
 #include "scene.h"
 
+#include "octree_gpu.h"
+
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -149,7 +151,7 @@ T *dev_upload(DeviceArena &a, const std::vector<T> &v) {
 
 }  // namespace
 
-SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
+SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode) {
   auto t_start = std::chrono::steady_clock::now();
   // ---- validation --------------------------------------------------------
   if (d.n_materials == 0 || !d.materials) fail("scene has no materials");
@@ -231,7 +233,26 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
     prims[3 * id + 2] = c;
     prim_mat[id] = mat;
   };
+  // The octree is built on the host (OctreeBuilder, surface by surface) or
+  // on the device (build_octree_device, the same tree from the surfaces'
+  // boxes in insertion order).
+  const bool dev_oct = upload && (octree_mode == SNOG_OCTREE_DEVICE ||
+                                  (octree_mode == SNOG_OCTREE_AUTO && n_prims >= kDeviceOctreeMinSurfaces));
   OctreeBuilder ob;
+  std::vector<Box3> oct_boxes;
+  std::vector<uint32_t> oct_refs;
+  if (dev_oct) {
+    oct_boxes.reserve(n_prims);
+    oct_refs.reserve(n_prims);
+  }
+  auto oct_add = [&](uint32_t ref, const Box3 &b) {
+    if (dev_oct) {
+      oct_boxes.push_back(b);
+      oct_refs.push_back(ref);
+    } else {
+      ob.add(ref, b);
+    }
+  };
   for (uint32_t v = 0; v < d.n_vertices; v++) mesh_box.add(v3(d.vertices + 3 * size_t(v)));
   for (uint32_t t = 0; t < d.n_triangles; t++) {
     const uint32_t *ix = d.triangles + 3 * size_t(t);
@@ -242,7 +263,7 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
         make_float4(e2.x, e2.y, e2.z, 0.f), d.tri_material[t]);
     // Degenerate triangles are left out of the space (surface/mesh.cc:833-846);
     // the mesh is left-handed, normal = e2 x e1 (surface/mesh.h:55).
-    if (vlen2(vcross(e2, e1)) > 0) ob.add(t, box_of_points({p0, p1, p2}));
+    if (vlen2(vcross(e2, e1)) > 0) oct_add(t, box_of_points({p0, p1, p2}));
   }
   if (d.n_triangles) scene_box.add(Box3{{mesh_box.lo[0], mesh_box.lo[1], mesh_box.lo[2]},
                                        {mesh_box.hi[0], mesh_box.hi[1], mesh_box.hi[2]}});
@@ -255,7 +276,7 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
     Box3 b{{s.center[0] - r, s.center[1] - r, s.center[2] - r},
            {s.center[0] + r, s.center[1] + r, s.center[2] + r}};   // surface/sphere.cc:164-170
     scene_box.add(b);
-    ob.add(id, b);
+    oct_add(id, b);
   }
   for (uint32_t i = 0; i < d.n_tripars; i++) {
     const SnogTripar &p = d.tripars[i];
@@ -266,9 +287,9 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
     Box3 b = p.parallelogram ? box_of_points({v0, vadd(v0, e1), vadd(v0, e2), vadd(vadd(v0, e1), e2)})
                              : box_of_points({v0, vadd(v0, e1), vadd(v0, e2)});   // surface/tripar.cc:188-197
     scene_box.add(b);
-    ob.add(id, b);
+    oct_add(id, b);
   }
-  S.oct = ob.finish();
+  if (!dev_oct) S.oct = ob.finish();
 
   // ---- light samplers, in the reference's order -------------------------
   std::vector<DevLight> lights;
@@ -410,10 +431,42 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
   std::memset(&D, 0, sizeof(D));
   DeviceArena &A = S.arena;
   if (upload) try {
-    std::vector<uint32_t> plist4;
-    std::vector<uint4> nodes = compact_nodes(S.oct, plist4);
-    D.nodes = dev_upload(A, nodes);
-    D.plist = dev_upload(A, plist4);
+    DeviceOctree dov;
+    bool built = false;
+    if (dev_oct) {
+      try {
+        build_octree_device(oct_boxes, oct_refs, A, dov);
+        built = true;
+      } catch (const Error &e) {
+        // Trees the device builder does not take (root grown more than 40
+        // times, deeper than 40 levels, or a descent wider than its stack)
+        // go to the host builder in AUTO mode.  The device builder finds
+        // these before it allocates its outputs in the scene's arena.
+        if (octree_mode != SNOG_OCTREE_AUTO || e.code != SNOG_EINVAL) throw;
+        for (size_t i = 0; i < oct_boxes.size(); i++) ob.add(oct_refs[i], oct_boxes[i]);
+        S.oct = ob.finish();
+      }
+    }
+    if (built) {
+      D.nodes = dov.nodes;
+      D.plist = dov.plist;
+      S.oct_device = true;
+      S.oct_nodes = dov.n_nodes;
+      S.oct_plist4 = dov.n_plist4;
+      S.oct.origin[0] = dov.origin[0];
+      S.oct.origin[1] = dov.origin[1];
+      S.oct.origin[2] = dov.origin[2];
+      S.oct.size = dov.size;
+      S.oct.max_depth = dov.max_depth;
+      S.oct.n_leaf = dov.n_leaf;
+      S.oct.n_list_surfaces = dov.n_list_surfaces;
+      S.oct_plist_host = dov.n_plist_host;
+    } else {
+      std::vector<uint32_t> plist4;
+      std::vector<uint4> nodes = compact_nodes(S.oct, plist4);
+      D.nodes = dev_upload(A, nodes);
+      D.plist = dev_upload(A, plist4);
+    }
     D.prims = dev_upload(A, prims);
     D.prim_mat = dev_upload(A, prim_mat);
     D.mats = dev_upload(A, mats);
@@ -427,7 +480,7 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
     throw;
   }
   S.on_device = upload;
-  D.n_nodes = uint32_t(S.oct.heads.size());
+  D.n_nodes = S.oct_device ? S.oct_nodes : uint32_t(S.oct.heads.size());
   D.n_tri = d.n_triangles;
   D.n_sph = d.n_spheres;
   D.n_tpar = d.n_tripars;
@@ -455,7 +508,7 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
   SnogSceneInfo &I = S.info;
   std::memset(&I, 0, sizeof(I));
   I.n_nodes = D.n_nodes;
-  I.n_plist = uint32_t(S.oct.plist.size());
+  I.n_plist = S.oct_device ? S.oct_plist_host : uint32_t(S.oct.plist.size());
   I.max_depth = S.oct.max_depth;
   I.n_leaf_nodes = S.oct.n_leaf;
   I.n_triangles = D.n_tri;
@@ -473,6 +526,16 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload) {
   I.device_bytes = A.bytes;
   I.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   return sc.release();
+}
+
+const OctreeArrays &host_octree(SceneImpl &S) {
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (S.oct_device && S.oct.heads.empty() && S.oct_nodes) {
+    check_cuda(cudaSetDevice(S.device), "cudaSetDevice");
+    S.oct = octree_from_device(S.dev.nodes, S.oct_nodes, S.dev.plist, S.oct_plist4, S.oct.origin, S.oct.size,
+                               S.oct.max_depth);
+  }
+  return S.oct;
 }
 
 }  // namespace snog

@@ -38,7 +38,10 @@ struct DeviceArena {
 struct SceneImpl {
   std::mutex mu;
   int device = 0;
-  OctreeArrays oct;                 // host copy (export, stats)
+  OctreeArrays oct;                 // host copy (export, stats); for a device-built
+                                    // tree only origin/size/statistics until exported
+  bool oct_device = false;          // the octree was built on the device
+  uint32_t oct_nodes = 0, oct_plist4 = 0, oct_plist_host = 0;
   DevScene dev{};                   // device view passed to kernels
   DeviceArena arena;
   SnogSceneInfo info{};
@@ -59,8 +62,18 @@ struct RenderPool {
 };
 RenderPool &render_pool(int device);
 
-// Build and upload; throws snog::Error on failure.
-SceneImpl *build_scene(const SnogSceneDesc &desc, bool upload = true);
+// Scenes with at least this many surfaces build their octree on the device
+// unless the caller asks for the host builder.
+constexpr size_t kDeviceOctreeMinSurfaces = 65536;
+
+// Build and upload; throws snog::Error on failure.  OCTREE_MODE is one of
+// SNOG_OCTREE_AUTO / _HOST / _DEVICE (a host-only scene always uses the host
+// builder).
+SceneImpl *build_scene(const SnogSceneDesc &desc, bool upload = true, uint32_t octree_mode = SNOG_OCTREE_AUTO);
+
+// The octree in the host layout, downloaded on first use for a device-built
+// tree.
+const OctreeArrays &host_octree(SceneImpl &S);
 
 struct Error {
   int code;

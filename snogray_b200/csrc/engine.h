@@ -207,7 +207,6 @@ class Engine {
   uint64_t next_id_ = 1;
   uint64_t pushed_tail_ = 0, pushed_cum_ = 0;
   uint64_t budget_used_ = 0;
-  size_t rr_ = 0;
   uint32_t kernel_launches_ = 0;
   uint64_t base_closest_ = 0, base_shadow_ = 0;
   std::chrono::steady_clock::time_point t0_;

@@ -200,11 +200,19 @@ __device__ __forceinline__ float4 *ring_slots() {
 }
 
 constexpr uint32_t kGateFlag = 8u;   // entry carries a parent gate
+constexpr uint32_t kSlowSlab = 8u;   // in Traversal::octant: slab bounds may be NaN
 
 __device__ __forceinline__ bool slab_open(float t0, float t1, float3 lo, float3 hi) {
   float min_t = fmax_ref(t0, fmax_ref(lo.x, fmax_ref(lo.y, lo.z)));
   float max_t = fmin_ref(t1, fmin_ref(hi.x, fmin_ref(hi.y, hi.z)));
   return !(min_t >= max_t);
+}
+
+// slab_open for bounds known to be NaN-free (finite slab, t0 and t1 not
+// NaN): maxima and minima are then exact and associative, so fmaxf / fminf
+// in any grouping decide the same as the reference's ordered ternaries.
+__device__ __forceinline__ bool slab_open_finite(float t0, float t1, float3 lo, float3 hi) {
+  return fmaxf(fmaxf(t0, lo.x), fmaxf(lo.y, lo.z)) < fminf(fminf(t1, hi.x), fminf(hi.y, hi.z));
 }
 
 // The parent's gate for a child with octant bits CB (parametric order), at
@@ -236,7 +244,7 @@ template <int STACK>
 struct Traversal {
   float3 o, d, lo, hi;
   float t0, t1;
-  uint32_t node, gate, octant, hit_ref;
+  uint32_t node, gate, octant, hit_ref;   // octant: bits 0-2, kSlowSlab
   uint32_t lp, lend;         // surface list still to test: plist[lp, lend)
   uint32_t ring;             // shared-memory ring: oldest position | count << 4 (0 when empty)
   int sp;                    // entries spilled to stk[0, sp)
@@ -279,6 +287,14 @@ struct Traversal {
     if (a > b) { float tmp = a; a = b; b = tmp; }
     lo.z = a; hi.z = b;
     octant = (d.x >= 0.f ? 0u : 4u) | (d.y >= 0.f ? 0u : 2u) | (d.z >= 0.f ? 0u : 1u);
+    // A node's bounds lie within its parent's (a far half's upper bound may
+    // round one ulp beyond): with every root bound below 1e37 in magnitude
+    // no bound below overflows, none is NaN, and with t0, t1 not NaN
+    // node_step may take its fast tests.  (fabsf(NaN) < x is false.)
+    const bool finite = fabsf(lo.x) < 1e37f && fabsf(lo.y) < 1e37f && fabsf(lo.z) < 1e37f &&
+                        fabsf(hi.x) < 1e37f && fabsf(hi.y) < 1e37f && fabsf(hi.z) < 1e37f && !isnan(t0) &&
+                        !isnan(t1);
+    if (!finite) octant |= kSlowSlab;
   }
 
   // The walk is over: no list pending, no current entry, empty stack.
@@ -342,14 +358,16 @@ struct Traversal {
   // tests, which only admits more children (the ray can only shrink), and
   // every entry's gate and cull are evaluated again when it is entered -- so
   // the tests and their order are the reference's.
+  template <bool FAST = true>
   __device__ __forceinline__ void node_step(TraceCounters &cnt) {
     if (!have && !pop()) return;
     have = false;
+    const bool slow = !FAST || (octant & kSlowSlab);
     bool open = true;
     if (gate & kGateFlag) open = gate_open(gate & 7u, t0, t1, lo, hi);
     if (open) {
       cnt.nodes++;
-      open = slab_open(t0, t1, lo, hi);
+      open = slow ? slab_open(t0, t1, lo, hi) : slab_open_finite(t0, t1, lo, hi);
     }
     if (!open) return;
     const uint4 nd = __ldg(nodes + node);
@@ -367,16 +385,39 @@ struct Traversal {
     const float3 near_lo = f3(__fadd_rn(lo.x, 0.f), __fadd_rn(lo.y, 0.f), __fadd_rn(lo.z, 0.f));
     // Which children pass gate and cull, by visiting position (bit i).  At
     // most 4 pass: one octant per crossing of each of the three midplanes.
+    const uint32_t oct = octant & 7u;
     uint32_t vm = 0;
+    if (slow) {
 #pragma unroll
-    for (uint32_t i = 0; i < 8; i++) {
-      const uint32_t cb = visit_bits(i);
-      const uint32_t slot = cb ^ octant;
-      const float3 clo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y,
-                            (cb & 1) ? mid.z : near_lo.z);
-      const float3 chi = f3((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z);
-      const bool ok = ((nd.y >> slot) & 1u) & gate_open(cb, t0, t1, clo, chi) & slab_open(t0, t1, clo, chi);
-      vm |= ok ? (1u << i) : 0u;
+      for (uint32_t i = 0; i < 8; i++) {
+        const uint32_t cb = visit_bits(i);
+        const uint32_t slot = cb ^ oct;
+        const float3 clo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y,
+                              (cb & 1) ? mid.z : near_lo.z);
+        const float3 chi = f3((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z);
+        const bool ok = ((nd.y >> slot) & 1u) & gate_open(cb, t0, t1, clo, chi) & slab_open(t0, t1, clo, chi);
+        vm |= ok ? (1u << i) : 0u;
+      }
+    } else {
+      // The same tests from shared pieces: per axis the near and far halves'
+      // gates, and the child's entry max(t0, lo.x, lo.y, lo.z) and exit
+      // min(t1, hi.x, hi.y, hi.z) built from an x part and a yz part.
+      const bool gx[2] = {t0 < mid.x, t1 > mid.x}, gy[2] = {t0 < mid.y, t1 > mid.y},
+                 gz[2] = {t0 < mid.z, t1 > mid.z};
+      const float in_x[2] = {fmaxf(t0, near_lo.x), fmaxf(t0, mid.x)};
+      const float out_x[2] = {fminf(t1, mid.x), fminf(t1, far.x)};
+      const float in_yz[4] = {fmaxf(near_lo.y, near_lo.z), fmaxf(near_lo.y, mid.z), fmaxf(mid.y, near_lo.z),
+                              fmaxf(mid.y, mid.z)};
+      const float out_yz[4] = {fminf(mid.y, mid.z), fminf(mid.y, far.z), fminf(far.y, mid.z), fminf(far.y, far.z)};
+#pragma unroll
+      for (uint32_t i = 0; i < 8; i++) {
+        const uint32_t cb = visit_bits(i);
+        const uint32_t bx = cb >> 2, by = (cb >> 1) & 1u, bz = cb & 1u;
+        const uint32_t slot = cb ^ oct;
+        const bool ok = ((nd.y >> slot) & 1u) & gx[bx] & gy[by] & gz[bz] &
+                        (fmaxf(in_x[bx], in_yz[2 * by + bz]) < fminf(out_x[bx], out_yz[2 * by + bz]));
+        vm |= ok ? (1u << i) : 0u;
+      }
     }
     if (!vm) return;
     // Every qualifying child but the first is pushed, in reverse visiting
@@ -386,7 +427,7 @@ struct Traversal {
       const uint32_t i = 31u - __clz(m);
       m &= ~(1u << i);
       const uint32_t cb = visit_bits(i);
-      const uint32_t slot = cb ^ octant;
+      const uint32_t slot = cb ^ oct;
       const uint32_t c = nd.x + __popc(nd.y & ((1u << slot) - 1u));
       push(make_float4((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y, (cb & 1) ? mid.z : near_lo.z,
                        __uint_as_float(c)),
@@ -396,7 +437,7 @@ struct Traversal {
     }
     const uint32_t i = __ffs(vm) - 1u;
     const uint32_t cb = visit_bits(i);
-    const uint32_t slot = cb ^ octant;
+    const uint32_t slot = cb ^ oct;
     node = nd.x + __popc(nd.y & ((1u << slot) - 1u));
     gate = cb | kGateFlag;
     lo = f3((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y, (cb & 1) ? mid.z : near_lo.z);
@@ -550,7 +591,7 @@ struct RayDispenser {
 // round of list entries pending, every live lane without a list pending
 // visits one octree entry; then the warp tests one round of pending list
 // entries together.  All 32 lanes of every warp must run it.
-template <int STACK, class Start, class Done>
+template <int STACK, bool FAST = true, class Start, class Done>
 __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, TraceCounters &cnt, Start start,
                                            Done done) {
   Traversal<STACK> tr;
@@ -571,7 +612,7 @@ __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, Trac
     // a round: list rounds run full, node steps run with more lanes at once.
     const uint32_t pend = (busy && tr.lp < tr.lend) ? tr.lend - tr.lp : 0u;
     const uint32_t pending = __reduce_add_sync(0xffffffffu, pend < 32u ? pend : 32u);
-    if (pending < 32u && busy && tr.lp >= tr.lend && !tr.finished()) tr.node_step(cnt);
+    if (pending < 32u && busy && tr.lp >= tr.lend && !tr.finished()) tr.template node_step<FAST>(cnt);
     const bool stop = list_round(tr, busy && tr.lp < tr.lend, any, cnt);
     if (busy && (stop || tr.finished())) {
       done(ray, tr, any);

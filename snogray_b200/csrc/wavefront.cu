@@ -156,7 +156,8 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_sha
   if (prof) warp_count(stats + 4, c.nodes, c.tests);
 }
 
-__global__ void __launch_bounds__(128) k_shade(DevScene s, JobConsts jc, uint64_t base, uint32_t bounce,
+// 6 blocks of 128 per SM (80 registers), as the engine's shading kernel.
+__global__ void __launch_bounds__(128, 6) k_shade(DevScene s, JobConsts jc, uint64_t base, uint32_t bounce,
                                                RayQ qin, uint32_t *counters, uint32_t cur,
                                                const uint32_t *hit_ref, const float *hit_t, PathPtrs P,
                                                RayQ qout, ShadowQ sq) {

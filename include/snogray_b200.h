@@ -94,6 +94,15 @@ typedef struct SnogSceneDesc {
   uint32_t env_width, env_height;                      /* 0 = none; width = 2*height */
   const float *env_rgb;                                /* env_height rows of env_width RGB, top row first */
   float env_frame[9];                                  /* envmap light frame axes x, y, z */
+  /* Optional vertex normals, 3 floats per vertex (NULL: none).  With them
+   * triangles shade with the interpolated normal and the geometric normal
+   * turned to agree with it (surface/mesh.cc:607-641, Mesh::add_normals
+   * mesh.h:95-111). */
+  const float *vertex_normals;
+  /* Nonzero for a right-handed mesh: geometric normal e1 x e2 instead of
+   * e2 x e1 (Mesh::left_handed, surface/mesh.cc:270; PLY meshes are
+   * right-handed, load/mesh/load-ply.cc). */
+  uint32_t mesh_right_handed;
 } SnogSceneDesc;
 
 /* Camera as the reference holds it after move/point/set_fov
@@ -158,6 +167,27 @@ int snog_init(int device);
  * Scene::light_samplers and EnvmapLight::Sampler's Hist2dDist
  * (light/envmap-light.cc:103-140, geometry/hist-2d-dist.cc:65-120). */
 int snog_scene_create(const SnogSceneDesc *desc, SnogScene **out);
+
+/* A triangle mesh read from a PLY file (ASCII, binary little- or
+ * big-endian), with the reference's rules (load/mesh/load-ply.cc:41-214):
+ * vertex x, y, z and optional nx, ny, nz properties, face vertex_indices
+ * lists of exactly 3 entries (faces with fewer are skipped, more are an
+ * error); a normal is kept only if some component exceeds 1e-15, and a later
+ * normal after a skipped one is an error ("Normal consistency error"); a
+ * face index goes through single precision as the reference's does.  The
+ * mesh is right-handed (set SnogSceneDesc::mesh_right_handed).  Arrays are
+ * owned by the library: release them with snog_ply_free. */
+typedef struct SnogPlyMesh {
+  uint32_t n_vertices;
+  float *vertices;           /* 3 per vertex */
+  float *normals;            /* 3 per vertex, or NULL */
+  uint32_t n_triangles;
+  uint32_t *triangles;       /* 3 per triangle */
+} SnogPlyMesh;
+
+/* Replaces load_ply_file (load/mesh/load-ply.cc:163-214). */
+int snog_ply_load(const char *path, SnogPlyMesh *out);
+int snog_ply_free(SnogPlyMesh *mesh);
 
 /* Octree builders for snog_scene_create_ex.  Both give the same tree (node
  * arrays and list order identical to Octree::Builder's); the device builder

@@ -235,6 +235,18 @@ class Mesh : public Surface {
     vertices.push_back(pos);
     return vert_index_t(vertices.size() - 1);
   }
+  // A vertex with its normal (Mesh::add_vertex (pos, normal), mesh.h:65-67);
+  // a mesh with normals shades with interpolated normals.
+  vert_index_t add_vertex(const Pos &pos, const Vec &normal) {
+    if (normals.size() != vertices.size()) throw std::runtime_error("Mesh: every vertex needs a normal");
+    normals.push_back(normal);
+    return add_vertex(pos);
+  }
+  // Normals for the vertices from BASE_VERT on (Mesh::add_normals, mesh.h:95-111).
+  void add_normals(const std::vector<Vec> &new_normals, vert_index_t base_vert) {
+    if (base_vert != normals.size()) throw std::runtime_error("Mesh::add_normals: normals out of step with vertices");
+    normals.insert(normals.end(), new_normals.begin(), new_normals.end());
+  }
   void add_triangle(part_index_t part, vert_index_t a, vert_index_t b, vert_index_t c) {
     at(part).tris.insert(at(part).tris.end(), {a, b, c});
   }
@@ -248,7 +260,9 @@ class Mesh : public Surface {
     std::vector<vert_index_t> tris;
   };
   std::vector<Pos> vertices;
+  std::vector<Vec> normals;        // empty, or one per vertex
   std::vector<Part> parts;
+  bool left_handed = true;         // geometric normal e2 x e1 (false: e1 x e2)
 
  private:
   Part &at(part_index_t p) {
@@ -256,6 +270,28 @@ class Mesh : public Surface {
     return parts[p];
   }
 };
+
+// load_ply_file (load/mesh/load-ply.cc:163-214): adds the PLY file's
+// vertices, normals and triangles (into PART) to MESH and makes it
+// right-handed, as the reference does.
+inline void load_ply_file(const std::string &filename, Mesh &mesh, Mesh::part_index_t part) {
+  SnogPlyMesh m{};
+  if (snog_ply_load(filename.c_str(), &m) != SNOG_OK) throw std::runtime_error(snog_last_error());
+  const Mesh::vert_index_t base = Mesh::vert_index_t(mesh.vertices.size());
+  const bool with_normals = m.normals != nullptr;
+  if (with_normals && mesh.normals.size() != mesh.vertices.size()) {
+    snog_ply_free(&m);
+    throw std::runtime_error("load_ply_file: the mesh's earlier vertices have no normals");
+  }
+  for (uint32_t v = 0; v < m.n_vertices; v++) {
+    mesh.vertices.push_back(Pos(m.vertices[3 * v], m.vertices[3 * v + 1], m.vertices[3 * v + 2]));
+    if (with_normals) mesh.normals.push_back(Vec(m.normals[3 * v], m.normals[3 * v + 1], m.normals[3 * v + 2]));
+  }
+  std::vector<Mesh::vert_index_t> idx(m.triangles, m.triangles + 3 * size_t(m.n_triangles));
+  snog_ply_free(&m);
+  mesh.add_triangles(part, idx, base);
+  mesh.left_handed = false;
+}
 
 // ---- lights ----------------------------------------------------------------
 
@@ -346,6 +382,8 @@ class GlobalRenderState {
     d.point_lights = f.plights.data();
     d.n_far_lights = uint32_t(f.flights.size());
     d.far_lights = f.flights.data();
+    d.vertex_normals = f.with_normals ? f.normals.data() : nullptr;
+    d.mesh_right_handed = f.left_handed ? 0u : 1u;
     if (f.env) {
       d.env_width = f.env->envmap->width;
       d.env_height = f.env->envmap->height;
@@ -381,8 +419,10 @@ class GlobalRenderState {
   struct Flat {
     std::vector<SnogMaterial> mats;
     std::map<const Material *, uint32_t> index;
-    std::vector<float> verts;
+    std::vector<float> verts, normals;
     std::vector<uint32_t> tris, tri_mat;
+    uint32_t n_meshes = 0;
+    bool with_normals = false, left_handed = true;
     std::vector<SnogSphere> spheres;
     std::vector<SnogTripar> tripars;
     std::vector<SnogPointLight> plights;
@@ -410,7 +450,17 @@ class GlobalRenderState {
       for (auto &s : g.surfaces)
         if (auto *mesh = dynamic_cast<const Mesh *>(s.get())) {
           const uint32_t base = uint32_t(verts.size() / 3);
+          // One mesh record per scene: every mesh must agree on handedness and
+          // on having vertex normals.
+          const bool has_n = !mesh->normals.empty();
+          if (n_meshes++ && (has_n != with_normals || mesh->left_handed != left_handed))
+            throw std::runtime_error("meshes of one scene must agree on handedness and vertex normals");
+          with_normals = has_n;
+          left_handed = mesh->left_handed;
+          if (has_n && mesh->normals.size() != mesh->vertices.size())
+            throw std::runtime_error("Mesh: normals for only some vertices");
           for (const Pos &p : mesh->vertices) verts.insert(verts.end(), {p.x, p.y, p.z});
+          for (const Vec &n : mesh->normals) normals.insert(normals.end(), {n.x, n.y, n.z});
           for (auto &part : mesh->parts) {
             uint32_t mi = mat(part.material);
             if (mi < last) {   // keep runs non-decreasing: a private copy of the record

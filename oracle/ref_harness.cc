@@ -14,6 +14,10 @@
 //                                   Octree::for_each_possible_intersector
 //                                   with the reference's own callbacks
 //                                   (space/space.cc:36-129)
+//   ply FILE OUT                    load a PLY mesh with load_ply_file
+//                                   (load/mesh/load-ply.cc) and dump its
+//                                   vertices, normals and triangles; a load
+//                                   error is written to OUT as its message
 //   render SPEC OUT.pfm [threads] [seed_skip] [spp] [row0] [rows] [repeat]
 //                                   RenderMgr::render of the whole image
 //                                   (render-mgr/render-mgr.cc:50-74), or of
@@ -71,6 +75,7 @@
 #include "light/envmap-light.h"
 #include "texture/envmap.h"
 #include "load/load-envmap.h"
+#include "load/mesh/load-ply.h"
 #include "image/image.h"
 #include "image/image-sampled-output.h"
 #include "camera/camera.h"
@@ -148,6 +153,8 @@ void build_scene(RefScene &rs, const std::string &spec_path) {
     Mesh *mesh = new Mesh();
     std::vector<scoord_t> vcoords(s.verts.begin(), s.verts.end());
     mesh->add_vertices(vcoords);
+    if (h.has_normals) mesh->add_normals(std::vector<sdist_t>(s.normals.begin(), s.normals.end()), 0);
+    mesh->left_handed = h.right_handed == 0;
     uint32_t t = 0;
     while (t < h.n_triangles) {
       uint32_t mat = s.tri_mat[t], t_end = t;
@@ -411,6 +418,43 @@ int mode_render(const std::string &spec, const std::string &out, unsigned thread
   return 0;
 }
 
+// OUT: "OK" or "ERR" + message line; for OK then uint32 n_vertices,
+// n_normals, n_triangles and the float / uint32 arrays.
+int mode_ply(const char *file, const char *out_path) {
+  Mesh mesh;
+  Mesh::part_index_t part = mesh.add_part(new Lambert(Color(0.5f)));
+  FILE *o = fopen(out_path, "wb");
+  if (!o) throw std::runtime_error("cannot write output");
+  try {
+    load_ply_file(file, mesh, part, ValTable());
+  } catch (std::exception &e) {
+    fprintf(o, "ERR %s\n", e.what());
+    fclose(o);
+    return 0;
+  }
+  fprintf(o, "OK\n");
+  const Mesh::Part &p = *mesh.parts[part];
+  uint32_t nv = uint32_t(mesh.vertices.size()), nn = uint32_t(mesh.vertex_normals.size()),
+           nt = uint32_t(p.triangles.size());
+  fwrite(&nv, 4, 1, o);
+  fwrite(&nn, 4, 1, o);
+  fwrite(&nt, 4, 1, o);
+  for (const auto &v : mesh.vertices) {
+    float c[3] = {float(v.x), float(v.y), float(v.z)};
+    fwrite(c, 4, 3, o);
+  }
+  for (const auto &v : mesh.vertex_normals) {
+    float c[3] = {float(v.x), float(v.y), float(v.z)};
+    fwrite(c, 4, 3, o);
+  }
+  for (const auto &t : p.triangles) {
+    uint32_t vi[3] = {uint32_t(t.vi[0]), uint32_t(t.vi[1]), uint32_t(t.vi[2])};
+    fwrite(vi, 4, 3, o);
+  }
+  fclose(o);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -418,6 +462,7 @@ int main(int argc, char **argv) {
     if (argc < 2) throw std::runtime_error("usage: snog_ref MODE ...");
     std::string mode = argv[1];
     if (mode == "octree" && argc == 4) return mode_octree(argv[2], argv[3]);
+    if (mode == "ply" && argc == 4) return mode_ply(argv[2], argv[3]);
     if (mode == "trace" && argc >= 5)
       return mode_trace(argv[2], argv[3], argv[4], argc > 5 ? atoi(argv[5]) : 1);
     if (mode == "render" && argc >= 4)

@@ -62,7 +62,9 @@ struct SpecHeader {
   uint32_t direct_samples;       // [surface_integ.direct_samples]
   float min_trace;               // [min_trace]
   float bg_alpha;                // [background_alpha]
-  uint32_t reserved[8];
+  uint32_t has_normals;          // vertex normals follow the envmap (3 floats each)
+  uint32_t right_handed;         // the mesh is right-handed (Mesh::left_handed false)
+  uint32_t reserved[6];
 };
 
 struct Scene {
@@ -76,6 +78,7 @@ struct Scene {
   std::vector<PointLightRec> plights;
   std::vector<FarLightRec> flights;
   std::vector<float> env;          // env_w*env_h*3, row 0 = top row of image
+  std::vector<float> normals;      // 3 per vertex when h.has_normals
 };
 
 template <class T>
@@ -102,6 +105,7 @@ static inline Scene load(const std::string &path) {
   read_vec(f, s.plights, s.h.n_point_lights);
   read_vec(f, s.flights, s.h.n_far_lights);
   read_vec(f, s.env, size_t(s.h.env_w) * s.h.env_h * 3);
+  if (s.h.has_normals) read_vec(f, s.normals, size_t(s.h.n_vertices) * 3);
   fclose(f);
   return s;
 }

@@ -71,7 +71,10 @@ def write_spec(path, scene, camera=None, params=None):
     hdr += np.array([params.width, params.height, params.spp, params.min_path_len,
                      params.max_path_len, params.direct_samples], "<u4").tobytes()
     hdr += np.array([params.min_trace, params.bg_alpha], "<f4").tobytes()
-    hdr += np.zeros(8, "<u4").tobytes()
+    normals = getattr(scene, "normals", None)
+    hdr += np.array([1 if normals is not None else 0, 1 if getattr(scene, "right_handed", False) else 0],
+                    "<u4").tobytes()
+    hdr += np.zeros(6, "<u4").tobytes()
     with open(path, "wb") as f:
         f.write(hdr)
         f.write(np.ascontiguousarray(scene.materials).tobytes())
@@ -84,6 +87,8 @@ def write_spec(path, scene, camera=None, params=None):
         f.write(np.ascontiguousarray(scene.far_lights).tobytes())
         if env is not None:
             f.write(np.ascontiguousarray(env, "<f4").tobytes())
+        if normals is not None:
+            f.write(np.ascontiguousarray(normals, "<f4").reshape(-1, 3).tobytes())
 
 
 def write_rays(path, soa, n_closest):
@@ -142,6 +147,27 @@ def ref_octree(scene, flavour="parity", tmpdir=None):
         oc = read_octree(op)
     oc["stats"] = stats
     return oc
+
+
+def ref_ply(path, flavour="parity", tmpdir=None):
+    """The reference's load_ply_file on PATH: {"vertices", "normals", "triangles"}
+    (normals: one row per normal the mesh kept) or {"error": message}."""
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        op = os.path.join(d, "p.bin")
+        _run([ref_binary(flavour), "ply", path, op])
+        with open(op, "rb") as f:
+            data = f.read()
+    head, _, rest = data.partition(b"\n")
+    if head.startswith(b"ERR"):
+        return {"error": head[4:].decode()}
+    nv, nn, nt = np.frombuffer(rest[:12], "<u4")
+    off = 12
+    verts = np.frombuffer(rest[off:off + 12 * nv], "<f4").reshape(nv, 3)
+    off += 12 * nv
+    nrm = np.frombuffer(rest[off:off + 12 * nn], "<f4").reshape(nn, 3)
+    off += 12 * nn
+    tris = np.frombuffer(rest[off:off + 12 * nt], "<u4").reshape(nt, 3)
+    return {"vertices": verts, "normals": nrm, "triangles": tris}
 
 
 def ref_trace(scene, soa, n_closest, threads=8, flavour="parity", tmpdir=None):

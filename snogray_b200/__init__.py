@@ -54,7 +54,14 @@ class SnogSceneDesc(C.Structure):
                 ("n_point_lights", C.c_uint32), ("point_lights", C.c_void_p),
                 ("n_far_lights", C.c_uint32), ("far_lights", C.c_void_p),
                 ("env_width", C.c_uint32), ("env_height", C.c_uint32),
-                ("env_rgb", C.c_void_p), ("env_frame", C.c_float * 9)]
+                ("env_rgb", C.c_void_p), ("env_frame", C.c_float * 9),
+                ("vertex_normals", C.c_void_p), ("mesh_right_handed", C.c_uint32)]
+
+
+class SnogPlyMesh(C.Structure):
+    _fields_ = [("n_vertices", C.c_uint32), ("vertices", C.POINTER(C.c_float)),
+                ("normals", C.POINTER(C.c_float)), ("n_triangles", C.c_uint32),
+                ("triangles", C.POINTER(C.c_uint32))]
 
 
 class SnogCamera(C.Structure):
@@ -230,6 +237,12 @@ class Scene:
             d.env_height, d.env_width = e.shape[0], e.shape[1]
             d.env_rgb = _ptr(e)
         d.env_frame[:] = [float(x) for x in np.asarray(data.env_frame, np.float32).reshape(9)]
+        if data.normals is not None:
+            nrm = arr(data.normals, np.float32)
+            if nrm.shape != data.vertices.shape:
+                raise ValueError("normals must have one (x, y, z) per vertex")
+            d.vertex_normals = _ptr(nrm)
+        d.mesh_right_handed = 1 if data.right_handed else 0
         h = _P()
         if device:
             _check(_scene_create_ex(C.byref(d), octree, C.byref(h)))
@@ -462,6 +475,29 @@ class Server:
             pass
 
 
+_ply_load = _sig("snog_ply_load", C.c_int, C.c_char_p, C.POINTER(SnogPlyMesh))
+_ply_free = _sig("snog_ply_free", C.c_int, C.POINTER(SnogPlyMesh))
+
+
+def load_ply(path):
+    """Read a PLY mesh with the reference's rules (snog_ply_load).  Returns
+    (vertices (n, 3) float32, normals (n, 3) float32 or None, triangles (m, 3)
+    uint32); the mesh is right-handed."""
+    m = SnogPlyMesh()
+    _check(_ply_load(os.fsencode(path), C.byref(m)))
+    try:
+        nv, nt = m.n_vertices, m.n_triangles
+        verts = np.ctypeslib.as_array(m.vertices, (nv * 3,)).reshape(nv, 3).copy() if nv else \
+            np.zeros((0, 3), np.float32)
+        nrm = (np.ctypeslib.as_array(m.normals, (nv * 3,)).reshape(nv, 3).copy()
+               if bool(m.normals) and nv else None)
+        tris = np.ctypeslib.as_array(m.triangles, (nt * 3,)).reshape(nt, 3).copy() if nt else \
+            np.zeros((0, 3), np.uint32)
+    finally:
+        _ply_free(C.byref(m))
+    return verts, nrm, tris
+
+
 def exported_symbols():
     """Names declared in include/snogray_b200.h (for the ABI check)."""
     import re
@@ -472,4 +508,4 @@ def exported_symbols():
 
 
 __all__ = ["Scene", "SceneData", "Camera", "RenderParams", "SnogError", "scenes", "init",
-           "version", "exported_symbols", "LIB_PATH"]
+           "version", "exported_symbols", "load_ply", "LIB_PATH"]

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "launch.h"
+#include "ply.h"
 #include "scene.h"
 
 namespace snog {
@@ -306,6 +307,40 @@ int snog_scene_destroy(SnogScene *scene) {
     }
     delete scene->impl;
     delete scene;
+    return int(SNOG_OK);
+  });
+}
+
+int snog_ply_load(const char *path, SnogPlyMesh *out) {
+  return guarded([&] {
+    if (!path || !out) throw Error{SNOG_EINVAL, "null argument"};
+    std::memset(out, 0, sizeof *out);
+    PlyMeshHost m = read_ply(path);
+    auto copy = [](const auto &v) {
+      using T = typename std::decay_t<decltype(v)>::value_type;
+      T *p = static_cast<T *>(std::malloc(v.empty() ? 1 : v.size() * sizeof(T)));
+      if (!p) throw std::bad_alloc();
+      if (!v.empty()) std::memcpy(p, v.data(), v.size() * sizeof(T));
+      return p;
+    };
+    SnogPlyMesh r{};
+    r.n_vertices = uint32_t(m.vertices.size() / 3);
+    r.n_triangles = uint32_t(m.triangles.size() / 3);
+    r.vertices = copy(m.vertices);
+    r.normals = m.normals.empty() ? nullptr : copy(m.normals);
+    r.triangles = copy(m.triangles);
+    *out = r;
+    return int(SNOG_OK);
+  });
+}
+
+int snog_ply_free(SnogPlyMesh *mesh) {
+  return guarded([&] {
+    if (!mesh) throw Error{SNOG_EINVAL, "null argument"};
+    std::free(mesh->vertices);
+    std::free(mesh->normals);
+    std::free(mesh->triangles);
+    std::memset(mesh, 0, sizeof *mesh);
     return int(SNOG_OK);
   });
 }

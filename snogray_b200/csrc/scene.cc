@@ -180,6 +180,9 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
       fail("envmap must be a lat-long image with width == 2 * height");
   }
   if (d.n_triangles + d.n_spheres + d.n_tripars == 0) fail("scene has no surfaces");
+  if (d.vertex_normals)
+    for (uint32_t v = 0; v < 3 * d.n_vertices; v++)
+      if (!std::isfinite(d.vertex_normals[v])) fail("vertex normal " + std::to_string(v / 3) + " is not finite");
   if (uint64_t(d.n_triangles) + d.n_spheres + d.n_tripars >= (1ull << 31))
     fail("too many primitives (limit 2^31)");
 
@@ -469,6 +472,17 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
     }
     D.prims = dev_upload(A, prims);
     D.prim_mat = dev_upload(A, prim_mat);
+    if (d.vertex_normals && d.n_triangles) {
+      std::vector<float4> vn(d.n_vertices);
+      for (uint32_t v = 0; v < d.n_vertices; v++)
+        vn[v] = make_float4(d.vertex_normals[3 * size_t(v)], d.vertex_normals[3 * size_t(v) + 1],
+                            d.vertex_normals[3 * size_t(v) + 2], 0.f);
+      std::vector<uint4> vi(d.n_triangles);
+      for (uint32_t t = 0; t < d.n_triangles; t++)
+        vi[t] = make_uint4(d.triangles[3 * size_t(t)], d.triangles[3 * size_t(t) + 1], d.triangles[3 * size_t(t) + 2], 0u);
+      D.vnormals = dev_upload(A, vn);
+      D.tri_vidx = dev_upload(A, vi);
+    }
     D.mats = dev_upload(A, mats);
     D.lights = dev_upload(A, lights);
     D.media = dev_upload(A, media);
@@ -504,6 +518,7 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
   D.size = S.oct.size;
   D.horizon = horizon;
   D.max_depth = S.oct.max_depth;
+  D.right_handed = d.mesh_right_handed ? 1u : 0u;
 
   SnogSceneInfo &I = S.info;
   std::memset(&I, 0, sizeof(I));

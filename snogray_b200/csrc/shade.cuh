@@ -154,25 +154,47 @@ __device__ __forceinline__ Isec make_isec(const DevScene &s, uint32_t ref, float
   I.pos = add(o, mul(d, t));
   const PrimRec r = load_prim(s, ref);
   I.mat = __ldg(s.prim_mat + ref);
-  Frame3 f;
+  Frame3 f, nf;
   if (r.a.w == float(PRIM_TRI)) {
-    f = tri_frame(s, I.pos, unit(cross(xyz(r.c), xyz(r.b))));
+    // Triangle::raw_normal: e2 x e1 for a left-handed mesh, e1 x e2 for a
+    // right-handed one (surface/mesh.cc:264-271), each in its own operand
+    // order (negating the other would flip the sign of zero components).
+    const float3 gn = unit(s.right_handed ? cross(xyz(r.b), xyz(r.c)) : cross(xyz(r.c), xyz(r.b)));
+    f = tri_frame(s, I.pos, gn);
+    nf = f;
+    if (s.vnormals) {
+      // Interpolated vertex normal at the hit's barycentrics (the same u, v
+      // the intersection test computed; they do not depend on the ray's
+      // extent), and the geometric normal turned to agree with it
+      // (surface/mesh.cc:616-637).
+      float th, u = 0.f, v = 0.f;
+      tripar_hit(xyz(r.a), xyz(r.b), xyz(r.c), false, o, d, -INFINITY, INFINITY, th, u, v);
+      const uint4 vi = __ldg(s.tri_vidx + ref);
+      float3 n = mul(xyz(__ldg(s.vnormals + vi.x)), 1.f - u - v);
+      n = add(n, mul(xyz(__ldg(s.vnormals + vi.y)), u));
+      n = add(n, mul(xyz(__ldg(s.vnormals + vi.z)), v));
+      n = unit(n);
+      if (dot(n, f.z) < 0.f) f.z = neg(f.z);
+      nf = tri_frame(s, I.pos, n);
+    }
   } else if (r.a.w == float(PRIM_SPHERE)) {
     float3 n = unit(sub(I.pos, xyz(r.a)));
     float3 tt = cross(n, f3(0.f, 0.f, 1.f));
     if (length_sq(tt) < 1e-15f) tt = perpendicular(n);
     tt = unit(tt);
     f = Frame3{tt, cross(tt, n), n};
+    nf = f;
   } else {
     float3 e1 = xyz(r.b), e2 = xyz(r.c);
     float3 n = unit(cross(e2, e1));
     float3 sx = mul(e1, 1.0f / length(e1));
     f = Frame3{sx, cross(sx, n), n};
+    nf = f;
   }
-  // normal frame == geometric frame (no vertex normals, no bump maps)
+  // Intersect::finish_init (render/intersect.cc:84-136); no bump maps.
   float3 wv = neg(unit(d));
-  I.nf = f;
-  I.v = f.to(wv);
+  I.nf = nf;
+  I.v = nf.to(wv);
   float gvz = dot(wv, f.z);
   I.back = gvz < 0.f;
   if (I.back) {

@@ -19,6 +19,8 @@
 //                     tripar    a = corner, b = edge1, c = edge2
 //                               a.w holds the kind (PRIM_* below, as a float)
 //   prim_mat       uint32[n_prims]        material index per primitive
+//   vnormals       float4[n_vertices]     vertex normals (optional), with
+//   tri_vidx       uint4[n_triangles]     each triangle's vertex indices
 //   mats, lights, envmap texels and Hist2dDist cumulative sums
 
 #ifndef SNOG_COMMON_H
@@ -106,7 +108,9 @@ struct DevScene {
   float mesh_center[3];       // midpoint of the mesh bounding box (mesh.cc:581)
   float horizon;              // scene bbox diameter (render/scene.cc:28)
   uint32_t max_depth;         // octree depth, sizes the traversal stack
-  uint32_t pad_;
+  uint32_t right_handed;      // mesh geometric normal e1 x e2 (else e2 x e1)
+  const float4 *vnormals;     // per vertex, or null: no interpolated normals
+  const uint4 *tri_vidx;      // per triangle, its vertex indices (with vnormals)
 };
 
 // -- float3 helpers --------------------------------------------------------

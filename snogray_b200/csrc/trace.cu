@@ -49,9 +49,11 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_BATCH_MINBLOCKS) k_tra
           float3 v = xsub(end, xyz(r.a));
           nv = xmul(v, __fdiv_rn(1.0f, __fsqrt_rn(xlen_sq(v))));
         } else {
-          // Triangles (left-handed mesh) and tripars: (e2 x e1).unit ()
-          // (surface/mesh.cc:713-718, surface/tripar.cc:78-82).
-          float3 v = xcross(xyz(r.c), xyz(r.b));
+          // Triangles: (e2 x e1).unit () for a left-handed mesh, (e1 x e2)
+          // for a right-handed one; tripars: e2 x e1 (surface/mesh.cc:264-271,
+          // 713-718, surface/tripar.cc:78-82).
+          const bool rh = r.a.w == float(PRIM_TRI) && s.right_handed;
+          float3 v = rh ? xcross(xyz(r.b), xyz(r.c)) : xcross(xyz(r.c), xyz(r.b));
           nv = xmul(v, __fdiv_rn(1.0f, __fsqrt_rn(xlen_sq(v))));
         }
       }

@@ -89,6 +89,8 @@ class SceneData:
     envmap: np.ndarray | None = None          # (H, W, 3) float32, row 0 = top
     env_frame: np.ndarray = field(default_factory=lambda: np.eye(3, dtype=np.float32))
     name: str = "scene"
+    normals: np.ndarray | None = None          # (n_vertices, 3) float32 vertex normals
+    right_handed: bool = False                 # mesh normal e1 x e2 (PLY meshes)
 
     def __post_init__(self):
         self.vertices = np.ascontiguousarray(self.vertices, np.float32).reshape(-1, 3)
@@ -98,6 +100,8 @@ class SceneData:
             raise ValueError("tri_mat must be non-decreasing (one mesh part per material run)")
         if self.envmap is not None:
             self.envmap = np.ascontiguousarray(self.envmap, np.float32)
+        if self.normals is not None:
+            self.normals = np.ascontiguousarray(self.normals, np.float32).reshape(-1, 3)
 
     @property
     def n_prims(self):
@@ -175,6 +179,85 @@ def cornell_camera(width, height):
 
 
 def cornell_params(width=256, height=256, spp=16, seed=0):
+    return RenderParams(width=width, height=height, spp=spp, min_path_len=3, max_path_len=8,
+                        direct_samples=1, seed=seed)
+
+
+# ---------------------------------------------------------------------------
+# Meshes as a PLY file gives them: right-handed (geometric normal e1 x e2),
+# optionally with vertex normals.  A UV sphere of radius 0.3 resting on a
+# floor quad, lit by a 0.5 x 0.5 area light; y up.
+
+def _uv_sphere(center, r, n_lng, n_lat):
+    """Vertices, outward unit normals and right-handed (counter-clockwise
+    seen from outside) triangles of a UV sphere."""
+    verts, nrms = [], []
+    for i in range(n_lat + 1):
+        th = math.pi * i / n_lat
+        for j in range(n_lng):
+            ph = 2 * math.pi * j / n_lng
+            n = (math.sin(th) * math.cos(ph), math.cos(th), math.sin(th) * math.sin(ph))
+            nrms.append(n)
+            verts.append(tuple(c + r * x for c, x in zip(center, n)))
+    tris = []
+    for i in range(n_lat):
+        for j in range(n_lng):
+            a, b = i * n_lng + j, i * n_lng + (j + 1) % n_lng
+            c, d = a + n_lng, b + n_lng
+            if i > 0:
+                tris.append([a, b, c])
+            if i < n_lat - 1:
+                tris.append([b, d, c])
+    return np.array(verts), np.array(nrms), tris
+
+
+def mesh_scene(smooth=True):
+    """SMOOTH: the sphere (Cook-Torrance) and floor (Lambert) carry vertex
+    normals.  Otherwise flat shading, the sphere is Glass and an emissive quad
+    faces the camera: both depend on which side the right-handed normal is."""
+    sv, sn, st = _uv_sphere((0.5, 0.3, 0.55), 0.3, 24, 12)
+    fv = np.array([[-0.5, 0, -0.5], [1.5, 0, -0.5], [1.5, 0, 1.5], [-0.5, 0, 1.5]])
+    fn = np.tile([[0.0, 1.0, 0.0]], (4, 1))
+    base = len(sv)
+    floor = [[base, base + 3, base + 2], [base, base + 2, base + 1]]   # e1 x e2 = +y
+    verts, nrms = [sv, fv], [sn, fn]
+    if smooth:
+        mats = _mats([material(MAT_LAMBERT, (0.6, 0.6, 0.6)),
+                      material(MAT_COOK_TORRANCE, (0.7, 0.3, 0.2), (1, 1, 1), m=0.2, ior_n=1.5),
+                      material(MAT_GLOW, (10.0, 10.0, 10.0))])
+        tris = floor + st
+        tri_mat = [0, 0] + [1] * len(st)
+    else:
+        mats = _mats([material(MAT_LAMBERT, (0.6, 0.6, 0.6)),
+                      material(MAT_GLASS, ior_n=1.5),
+                      material(MAT_GLOW, (4.0, 3.0, 2.0)),
+                      material(MAT_GLOW, (10.0, 10.0, 10.0))])
+        qb = base + 4
+        qv = np.array([[-0.2, 0.1, 0.9], [0.1, 0.1, 0.9], [0.1, 0.6, 0.9], [-0.2, 0.6, 0.9]])
+        verts.append(qv)
+        nrms.append(np.tile([[0.0, 0.0, -1.0]], (4, 1)))
+        quad = [[qb, qb + 2, qb + 1], [qb, qb + 3, qb + 2]]   # e1 x e2 = -z, towards the camera
+        tris = floor + st + quad
+        tri_mat = [0, 0] + [1] * len(st) + [2, 2]
+    tripars = np.zeros(1, TRIPAR_DTYPE)
+    tripars[0] = ((0.25, 1.2, 0.25), (0, 0, 0.5), (0.5, 0, 0), 1, len(mats) - 1)   # e2 x e1 = -y
+    v = np.concatenate(verts).astype(np.float32)
+    n = np.concatenate(nrms).astype(np.float32)
+    return SceneData(materials=mats, vertices=v, triangles=np.array(tris, np.uint32),
+                     tri_mat=np.array(tri_mat, np.uint32), tripars=tripars,
+                     normals=n if smooth else None, right_handed=True,
+                     name="mesh_smooth" if smooth else "mesh_flat")
+
+
+def mesh_camera(width, height):
+    cam = Camera()
+    cam.move((0.5, 0.55, -1.3))
+    cam.point((0.5, 0.3, 0.5), (0, 1, 0))
+    cam.set_vert_fov(math.radians(45.0), width / height)
+    return cam
+
+
+def mesh_params(width=64, height=64, spp=16, seed=0):
     return RenderParams(width=width, height=height, spp=spp, min_path_len=3, max_path_len=8,
                         direct_samples=1, seed=seed)
 
@@ -266,6 +349,10 @@ def scene_digest(sd):
         h.update(np.ascontiguousarray(a).tobytes())
     if sd.envmap is not None:
         h.update(np.ascontiguousarray(sd.envmap).tobytes())
+    if sd.normals is not None:
+        h.update(np.ascontiguousarray(sd.normals).tobytes())
+    if sd.right_handed:
+        h.update(b"right-handed")
     return h.hexdigest()
 
 

@@ -99,6 +99,11 @@ TRACE_CASES = {
     "cornell_camera": (lambda: scenes.cornell_box(),
                        lambda sd: camera_rays(scenes.cornell_camera(64, 64), 64, 64,
                                               np.float32(4.0), seed=41)),
+    # a right-handed mesh (PLY convention): normals e1 x e2
+    "mesh_flat": (lambda: scenes.mesh_scene(smooth=False),
+                  lambda sd: np.concatenate([camera_rays(scenes.mesh_camera(48, 48), 48, 48,
+                                                         np.float32(4.0), seed=43),
+                                             edge_rays(sd, 4000, seed=47)], 1)),
 }
 
 
@@ -134,6 +139,11 @@ RENDER_CASES = {
     "cornell": (scenes.cornell_box, scenes.cornell_camera, scenes.cornell_params, 128, 128, 16),
     "terrain": (lambda: scenes.terrain_scene(n=96, n_spheres=40, seed=11, env_w=256, env_h=128),
                 scenes.terrain_camera, scenes.terrain_params, 64, 48, 16),
+    # right-handed meshes, with vertex normals and flat
+    "mesh_smooth": (lambda: scenes.mesh_scene(smooth=True), scenes.mesh_camera, scenes.mesh_params,
+                    64, 64, 16),
+    "mesh_flat": (lambda: scenes.mesh_scene(smooth=False), scenes.mesh_camera, scenes.mesh_params,
+                  64, 64, 16),
 }
 
 
@@ -168,6 +178,9 @@ if __name__ == "__main__":
             gen_trace(nm)
     if "render" in which:
         for nm in RENDER_CASES:
+            gen_render(nm)
+    for nm in which:
+        if nm in RENDER_CASES:
             gen_render(nm)
     with open(os.path.join(HERE, "README.txt"), "w") as f:
         f.write("Golden fixtures made by tests/golden/gen_golden.py from the snogray reference\n"

@@ -59,6 +59,8 @@ def fp64_t_and_normal(sd, rays, prim):
             tp = sd.tripars[p - nt - ns]
             corner, e1, e2 = (tp[k].astype(np.float64) for k in ("v0", "e1", "e2"))
         nn = np.cross(e2, e1)
+        if p < nt and sd.right_handed:
+            nn = -nn                                # right-handed mesh: e1 x e2
         pv = np.cross(d[i], e2)
         det = e1 @ pv
         q = np.cross(o[i] - corner, e1)

@@ -331,6 +331,25 @@ int snog_server_poll(SnogServer *server, uint64_t job_id, SnogJobStats *stats);
 /* Wait up to timeout_ms; SNOG_ETIMEOUT if the job is still running. */
 int snog_server_wait(SnogServer *server, uint64_t job_id, uint32_t timeout_ms, SnogJobStats *stats);
 int snog_server_cancel(SnogServer *server, uint64_t job_id);
+
+/* Preemption and checkpoints of resident jobs; replaces the reference's
+ * recovery of an interrupted render (--continue: image/recover-image.cc:32-88,
+ * snogray.lua:466-486), at path granularity.
+ * snog_server_pause stops starting a job's paths (those started finish) and
+ * frees the device for other jobs; snog_server_resume continues it.  A job
+ * stays SNOG_EBUSY while paused and keeps its per-job device memory. */
+int snog_server_pause(SnogServer *server, uint64_t job_id);
+int snog_server_resume(SnogServer *server, uint64_t job_id);
+/* Write a paused job's finished paths (per-path radiance and film jitter,
+ * with its camera and parameters) to PATH, once none is in flight (waits up
+ * to TIMEOUT_MS: SNOG_ETIMEOUT).  The job stays paused. */
+int snog_server_checkpoint(SnogServer *server, uint64_t job_id, const char *path, uint32_t timeout_ms);
+/* Submit a job continuing the checkpoint in PATH on the scene in SLOT (the
+ * scene it was taken on; SNOG_EINVAL otherwise): only the remaining paths
+ * are traced, and the image is the one an uninterrupted render of the job
+ * gives (path streams are keyed by job seed and path index). */
+int snog_server_submit_resume(SnogServer *server, uint32_t slot, const char *path, float *host_out,
+                              uint64_t *job_id);
 /* Stops the server thread (finishing nothing further) and frees it. */
 int snog_server_destroy(SnogServer *server);
 

@@ -163,6 +163,11 @@ _server_submit = _sig("snog_server_submit", C.c_int, _P, C.c_uint32, C.POINTER(S
 _server_poll = _sig("snog_server_poll", C.c_int, _P, C.c_uint64, C.POINTER(SnogJobStats))
 _server_wait = _sig("snog_server_wait", C.c_int, _P, C.c_uint64, C.c_uint32, C.POINTER(SnogJobStats))
 _server_cancel = _sig("snog_server_cancel", C.c_int, _P, C.c_uint64)
+_server_pause = _sig("snog_server_pause", C.c_int, _P, C.c_uint64)
+_server_resume = _sig("snog_server_resume", C.c_int, _P, C.c_uint64)
+_server_checkpoint = _sig("snog_server_checkpoint", C.c_int, _P, C.c_uint64, C.c_char_p, C.c_uint32)
+_server_submit_resume = _sig("snog_server_submit_resume", C.c_int, _P, C.c_uint32, C.c_char_p,
+                             C.c_void_p, C.POINTER(C.c_uint64))
 _server_destroy = _sig("snog_server_destroy", C.c_int, _P)
 
 
@@ -456,6 +461,29 @@ class Server:
 
     def cancel(self, job):
         _check(_server_cancel(self._h, job))
+
+    def pause(self, job):
+        """Stop starting JOB's paths; those in flight finish (snog_server_pause)."""
+        _check(_server_pause(self._h, job))
+
+    def resume(self, job):
+        _check(_server_resume(self._h, job))
+
+    def checkpoint(self, job, path, timeout_ms=60000):
+        """Write paused JOB's finished paths to PATH (snog_server_checkpoint)."""
+        _check(_server_checkpoint(self._h, job, os.fsencode(path), timeout_ms))
+
+    def submit_resume(self, slot, path):
+        """A job continuing the checkpoint in PATH; its image goes where
+        wait() returns it, like submit()."""
+        with open(path, "rb") as f:
+            head = f.read(8 + C.sizeof(SnogCamera) + C.sizeof(SnogRenderParams))
+        ps = SnogRenderParams.from_buffer_copy(head[8 + C.sizeof(SnogCamera):])
+        out = np.empty((ps.height, ps.width, 3), np.float32)
+        jid = C.c_uint64()
+        _check(_server_submit_resume(self._h, slot, os.fsencode(path), out.ctypes.data, C.byref(jid)))
+        self._outs[jid.value] = out
+        return jid.value
 
     def close(self):
         if getattr(self, "_h", None):

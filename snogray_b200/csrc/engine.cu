@@ -584,8 +584,13 @@ void Engine::build_graph() {
   check_cuda(e, "graph instantiate");
 }
 
+uint64_t Engine::scene_check(uint32_t scene_slot) const {
+  const DevScene &d = scenes_.at(scene_slot)->dev;
+  return uint64_t(d.n_tri + d.n_sph + d.n_tpar) | (uint64_t(d.n_nodes) << 32);
+}
+
 uint64_t Engine::submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRenderParams &p, float *out,
-                        bool out_on_device, double submit_ms) {
+                        bool out_on_device, double submit_ms, Checkpoint *resume) {
   if (scene_slot >= scenes_.size()) throw Error{SNOG_ENOTFOUND, "unknown scene slot"};
   if (p.width == 0 || p.height == 0 || p.spp == 0) throw Error{SNOG_EINVAL, "width, height, spp must be > 0"};
   if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};
@@ -606,10 +611,54 @@ uint64_t Engine::submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRe
   if (j.bytes > cfg_.mem_budget) throw Error{SNOG_ENOMEM, "job larger than the engine's memory budget"};
   j.st.submit_ms = submit_ms >= 0 ? submit_ms : now_ms();
   j.st.paths = uint64_t(p.width) * p.height * p.spp;
+  j.cam = cam;
+  j.params = p;
+  if (resume) {
+    if (resume->total != j.total || resume->done > j.total || resume->result.size() != resume->done ||
+        resume->jit.size() != resume->done)
+      throw Error{SNOG_EINVAL, "checkpoint does not match the job's size"};
+    if (resume->scene_check != scene_check(scene_slot))
+      throw Error{SNOG_EINVAL, "checkpoint was taken on a different scene"};
+    j.resume.reset(new Checkpoint(std::move(*resume)));
+  }
   const uint64_t id = j.id;
-  jobs_.emplace(id, j);
+  jobs_.emplace(id, std::move(j));
   pending_.push_back(id);
   return id;
+}
+
+bool Engine::pause(uint64_t id, bool on) {
+  auto it = jobs_.find(id);
+  if (it == jobs_.end()) return false;
+  it->second.paused = on;
+  return true;
+}
+
+bool Engine::drained(uint64_t id) const {
+  auto it = jobs_.find(id);
+  if (it == jobs_.end()) return false;
+  const HostJob &j = it->second;
+  return j.paused && j.table_slot != ~0u && done_host_[j.table_slot] >= j.pushed;
+}
+
+void Engine::checkpoint(uint64_t id, Checkpoint &out) {
+  if (!drained(id)) throw Error{SNOG_EBUSY, "job is not paused with its paths finished"};
+  HostJob &j = jobs_.at(id);
+  out.cam = j.cam;
+  out.params = j.params;
+  out.total = j.total;
+  out.done = j.pushed;
+  out.scene_check = scene_check(j.scene_slot);
+  out.result.resize(j.pushed);
+  out.jit.resize(j.pushed);
+  if (j.pushed) {
+    check_cuda(cudaMemcpyAsync(out.result.data(), j.result, j.pushed * sizeof(float4), cudaMemcpyDeviceToHost,
+                               stream_),
+               "checkpoint");
+    check_cuda(cudaMemcpyAsync(out.jit.data(), j.jit, j.pushed * sizeof(float2), cudaMemcpyDeviceToHost, stream_),
+               "checkpoint");
+  }
+  check_cuda(cudaStreamSynchronize(stream_), "checkpoint");
 }
 
 bool Engine::cancel(uint64_t id) {
@@ -694,6 +743,24 @@ void Engine::admit() {
                "job record");
     check_cuda(cudaMemsetAsync(job_done_ + j.table_slot, 0, 8, stream_), "job counter");
     done_host_[j.table_slot] = 0;
+    if (j.resume) {
+      // A resumed job: its finished paths come from the checkpoint and
+      // count as done; work items start after them.
+      const Checkpoint &c = *j.resume;
+      if (c.done) {
+        check_cuda(cudaMemcpyAsync(j.result, c.result.data(), c.done * sizeof(float4), cudaMemcpyHostToDevice,
+                                   stream_),
+                   "resume");
+        check_cuda(cudaMemcpyAsync(j.jit, c.jit.data(), c.done * sizeof(float2), cudaMemcpyHostToDevice, stream_),
+                   "resume");
+        const unsigned long long done = c.done;
+        check_cuda(cudaMemcpyAsync(job_done_ + j.table_slot, &done, 8, cudaMemcpyHostToDevice, stream_), "resume");
+        check_cuda(cudaStreamSynchronize(stream_), "resume");
+      }
+      j.pushed = c.done;
+      done_host_[j.table_slot] = c.done;
+      j.resume.reset();
+    }
     j.st.admit_ms = now_ms();
     active_.push_back(j.id);
     pending_.pop_front();
@@ -732,7 +799,7 @@ void Engine::push_items() {
   for (int pass = 0; pass < 2; pass++) {   // small jobs, then all jobs, each in arrival order
     for (size_t k = 0; k < active_.size() && room(); k++) {
       HostJob &j = jobs_.at(active_[k]);
-      if (j.canceled || (pass == 0 && j.total > small)) continue;
+      if (j.canceled || j.paused || (pass == 0 && j.total > small)) continue;
       while (j.pushed < j.total && room()) push_from(j);
     }
   }
@@ -777,7 +844,22 @@ bool Engine::step() {
   // After a launch (an even number of iterations) the live rays are in queue 0.
   const bool inflight = last_ctl_.qcount[0] > 0 || last_ctl_.ticket < pushed_cum_;
   if (!inflight && active_.empty() && pending_.empty()) return false;
-  if (inflight || !active_.empty()) {
+  // Launch while paths are in flight or an active job has work to push; a
+  // job complete on the device is finished below either way.
+  bool work = inflight;
+  for (size_t k = 0; k < active_.size() && !work; k++) {
+    const HostJob &j = jobs_.at(active_[k]);
+    work = !j.paused && !j.canceled && j.pushed < j.total;
+  }
+  bool finishing = false;
+  for (size_t k = 0; k < active_.size() && !finishing; k++) {
+    const HostJob &j = jobs_.at(active_[k]);
+    finishing = done_host_[j.table_slot] >= j.total || (j.canceled && done_host_[j.table_slot] >= j.pushed);
+  }
+  // Nothing to launch or finish: every remaining job is paused (or waits
+  // for memory a paused job holds).  The caller waits for a command.
+  if (!work && !finishing) return false;
+  if (work) {
     if (profile_on_) {
       launch_iterations();
     } else {

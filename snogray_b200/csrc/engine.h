@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -125,11 +126,35 @@ class Engine {
   void set_profile(bool on) { profile_on_ = on; }
   const Profile &profile() const { return prof_; }
   void clear_counters();
+  // A job's finished paths [0, done): per-path radiance + alpha and film
+  // jitter, with the job's camera and parameters -- what a resumed job needs.
+  struct Checkpoint {
+    SnogCamera cam{};
+    SnogRenderParams params{};
+    uint64_t total = 0, done = 0;
+    uint64_t scene_check = 0;           // primitive and octree node counts of the scene
+    std::vector<float4> result;
+    std::vector<float2> jit;
+  };
   // Queue a job; OUT is a host (on_device = false) or device image buffer.
   // SUBMIT_MS (engine clock) overrides the submission time recorded.
+  // RESUME (optional): continue from a checkpoint of the same camera and
+  // parameters on the same scene; its paths are not traced again.
   uint64_t submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRenderParams &p, float *out,
-                  bool out_on_device, double submit_ms = -1);
+                  bool out_on_device, double submit_ms = -1, Checkpoint *resume = nullptr);
   bool cancel(uint64_t job);
+  // Stop (PAUSE) or restart pushing a job's work; paths already pushed finish.
+  bool pause(uint64_t job, bool pause);
+  bool is_paused(uint64_t job) const {
+    auto it = jobs_.find(job);
+    return it != jobs_.end() && it->second.paused;
+  }
+  // True when JOB is paused, admitted and has no path in flight.
+  bool drained(uint64_t job) const;
+  // Copy a drained job's finished paths out (throws if not drained).
+  void checkpoint(uint64_t job, Checkpoint &out);
+  // Scene fingerprint recorded in checkpoints.
+  uint64_t scene_check(uint32_t scene_slot) const;
   // Drive the engine until every submitted job is finished (batch mode).
   void run_to_completion();
   // One scheduling round: admit, push items, one graph launch, completions.
@@ -159,6 +184,10 @@ class Engine {
     float *dev_out = nullptr;
     uint64_t bytes = 0;
     bool canceled = false, cancel_sent = false;
+    bool paused = false;
+    SnogCamera cam{};
+    SnogRenderParams params{};
+    std::unique_ptr<Checkpoint> resume;   // uploaded at admission, then dropped
     JobStatsHost st;
   };
 

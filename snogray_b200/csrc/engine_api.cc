@@ -7,6 +7,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <condition_variable>
 #include <cstring>
@@ -14,6 +16,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -180,6 +183,21 @@ struct SnogServer {
   };
   std::deque<Inbox> inbox;
   std::vector<uint64_t> cancels;
+  std::vector<std::pair<uint64_t, bool>> pauses;      // (server id, pause) requests
+  std::set<uint64_t> pause_requested;                  // server ids paused by the caller
+  // Checkpoint requests, filled by the worker between scheduling rounds once
+  // the job has no path in flight (API threads never take engine_mu while
+  // the worker runs: it would re-take the mutex first every round).
+  struct CkpReq {
+    uint64_t job;
+    bool done = false;
+    std::string error;
+    Engine::Checkpoint data;
+  };
+  std::vector<std::shared_ptr<CkpReq>> ckp_reqs;
+  bool ckp_new = false;
+  std::map<uint64_t, std::unique_ptr<Engine::Checkpoint>> resumes;   // inbox id -> checkpoint
+  bool idle = false;                                   // last step found nothing to run
   std::unordered_map<uint64_t, uint64_t> to_engine;   // server id -> engine id
   std::map<uint64_t, JobStatsHost> results;           // finished
   std::map<uint64_t, std::string> failed;             // refused at admission
@@ -189,20 +207,35 @@ struct SnogServer {
     for (;;) {
       std::vector<Inbox> take;
       std::vector<uint64_t> cancel_now;
+      std::vector<std::pair<uint64_t, bool>> pause_now;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return stop || !inbox.empty() || !to_engine.empty() || !cancels.empty(); });
+        cv_work.wait(lk, [&] {
+          return stop || !inbox.empty() || !cancels.empty() || !pauses.empty() || ckp_new ||
+                 (!to_engine.empty() && !idle);
+        });
+        ckp_new = false;
         if (stop) return;
         take.assign(inbox.begin(), inbox.end());
         inbox.clear();
         cancel_now.swap(cancels);
+        pause_now.swap(pauses);
       }
       std::vector<std::pair<uint64_t, JobStatsHost>> finished;
       try {
         std::lock_guard<std::mutex> elk(engine_mu);
         for (auto &in : take) {
           try {
-            uint64_t eid = engine->submit(in.slot, in.cam, in.p, in.out, false, in.submit_ms);
+            std::unique_ptr<Engine::Checkpoint> ck;
+            {
+              std::lock_guard<std::mutex> lk(mu);
+              auto r = resumes.find(in.id);
+              if (r != resumes.end()) {
+                ck = std::move(r->second);
+                resumes.erase(r);
+              }
+            }
+            uint64_t eid = engine->submit(in.slot, in.cam, in.p, in.out, false, in.submit_ms, ck.get());
             std::lock_guard<std::mutex> lk(mu);
             to_engine[in.id] = eid;
           } catch (const Error &e) {
@@ -215,8 +248,27 @@ struct SnogServer {
           auto it = to_engine.find(id);
           if (it != to_engine.end()) engine->cancel(it->second);
         }
-        engine->step();
+        for (auto &pr : pause_now) {
+          std::lock_guard<std::mutex> lk(mu);
+          auto it = to_engine.find(pr.first);
+          if (it != to_engine.end()) engine->pause(it->second, pr.second);
+        }
+        const bool ran = engine->step();
         std::lock_guard<std::mutex> lk(mu);
+        idle = !ran;
+        for (auto r = ckp_reqs.begin(); r != ckp_reqs.end();) {
+          auto t = to_engine.find((*r)->job);
+          if (t == to_engine.end()) {
+            (*r)->error = "job is over; nothing to checkpoint";
+          } else if (engine->drained(t->second)) {
+            engine->checkpoint(t->second, (*r)->data);
+          } else {
+            ++r;
+            continue;
+          }
+          (*r)->done = true;
+          r = ckp_reqs.erase(r);
+        }
         for (auto it = to_engine.begin(); it != to_engine.end();) {
           JobStatsHost s = engine->stats(it->second);
           if (s.status != SNOG_EBUSY) {
@@ -422,6 +474,60 @@ int snog_server_submit(SnogServer *server, uint32_t slot, const SnogCamera *came
   });
 }
 
+// Pause / resume requests go to the worker, which applies them between
+// scheduling rounds.
+static int server_pause(SnogServer *server, uint64_t job_id, bool on) {
+  return api_call([&] {
+    if (!server) throw Error{SNOG_EINVAL, "null argument"};
+    {
+      std::lock_guard<std::mutex> lk(server->mu);
+      if (job_id == 0 || job_id >= server->next_id) throw Error{SNOG_ENOTFOUND, "unknown job"};
+      if (server->results.count(job_id) || server->failed.count(job_id))
+        throw Error{SNOG_EINVAL, "job is over"};
+      if (on) server->pause_requested.insert(job_id);
+      else server->pause_requested.erase(job_id);
+      server->pauses.push_back({job_id, on});
+    }
+    server->cv_work.notify_one();
+    return int(SNOG_OK);
+  });
+}
+
+// Checkpoint file: "SNOGCKP1", the job's SnogCamera and SnogRenderParams,
+// uint64 total paths, finished paths D, scene fingerprint, then D float4
+// (radiance, alpha) and D float2 (film jitter), little-endian.
+static void write_checkpoint(const char *path, const Engine::Checkpoint &c) {
+  FILE *f = std::fopen(path, "wb");
+  if (!f) throw Error{SNOG_EINVAL, std::string("cannot write ") + path};
+  bool ok = std::fwrite("SNOGCKP1", 1, 8, f) == 8 && std::fwrite(&c.cam, sizeof c.cam, 1, f) == 1 &&
+            std::fwrite(&c.params, sizeof c.params, 1, f) == 1 && std::fwrite(&c.total, 8, 1, f) == 1 &&
+            std::fwrite(&c.done, 8, 1, f) == 1 && std::fwrite(&c.scene_check, 8, 1, f) == 1 &&
+            std::fwrite(c.result.data(), sizeof(float4), c.done, f) == c.done &&
+            std::fwrite(c.jit.data(), sizeof(float2), c.done, f) == c.done;
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) throw Error{SNOG_EINVAL, std::string("writing ") + path + " failed"};
+}
+
+static Engine::Checkpoint read_checkpoint(const char *path) {
+  FILE *f = std::fopen(path, "rb");
+  if (!f) throw Error{SNOG_EINVAL, std::string("cannot read ") + path};
+  Engine::Checkpoint c;
+  char magic[8];
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "SNOGCKP1", 8) == 0 &&
+            std::fread(&c.cam, sizeof c.cam, 1, f) == 1 && std::fread(&c.params, sizeof c.params, 1, f) == 1 &&
+            std::fread(&c.total, 8, 1, f) == 1 && std::fread(&c.done, 8, 1, f) == 1 &&
+            std::fread(&c.scene_check, 8, 1, f) == 1 && c.done <= c.total && c.done <= (1ull << 32);
+  if (ok) {
+    c.result.resize(c.done);
+    c.jit.resize(c.done);
+    ok = std::fread(c.result.data(), sizeof(float4), c.done, f) == c.done &&
+         std::fread(c.jit.data(), sizeof(float2), c.done, f) == c.done;
+  }
+  std::fclose(f);
+  if (!ok) throw Error{SNOG_EINVAL, std::string(path) + " is not a complete snogray_b200 checkpoint"};
+  return c;
+}
+
 static int server_status(SnogServer *server, uint64_t job_id, SnogJobStats *stats) {
   auto r = server->results.find(job_id);
   if (r != server->results.end()) {
@@ -481,6 +587,64 @@ int snog_server_cancel(SnogServer *server, uint64_t job_id) {
       // Running, or taken by the worker and about to be: the worker applies
       // cancels after the submissions it has taken.
       server->cancels.push_back(job_id);
+    }
+    server->cv_work.notify_one();
+    return int(SNOG_OK);
+  });
+}
+
+int snog_server_pause(SnogServer *server, uint64_t job_id) { return server_pause(server, job_id, true); }
+
+int snog_server_resume(SnogServer *server, uint64_t job_id) { return server_pause(server, job_id, false); }
+
+int snog_server_checkpoint(SnogServer *server, uint64_t job_id, const char *path, uint32_t timeout_ms) {
+  return api_call([&] {
+    if (!server || !path) throw Error{SNOG_EINVAL, "null argument"};
+    auto req = std::make_shared<SnogServer::CkpReq>();
+    req->job = job_id;
+    {
+      std::lock_guard<std::mutex> lk(server->mu);
+      auto fin = server->results.find(job_id);
+      if (fin != server->results.end())
+        throw Error{SNOG_EINVAL, fin->second.status == SNOG_OK ? "job is finished; nothing to checkpoint"
+                                                               : "job was cancelled or refused; nothing to checkpoint"};
+      auto bad = server->failed.find(job_id);
+      if (bad != server->failed.end()) throw Error{SNOG_EINVAL, "job failed: " + bad->second};
+      if (job_id == 0 || job_id >= server->next_id) throw Error{SNOG_ENOTFOUND, "unknown job"};
+      if (!server->pause_requested.count(job_id)) throw Error{SNOG_EINVAL, "job is not paused (snog_server_pause)"};
+      server->ckp_reqs.push_back(req);
+      server->ckp_new = true;
+    }
+    server->cv_work.notify_one();
+    {
+      std::unique_lock<std::mutex> lk(server->mu);
+      const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+      while (!req->done) {
+        if (server->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !req->done) {
+          auto &v = server->ckp_reqs;
+          v.erase(std::remove(v.begin(), v.end(), req), v.end());
+          throw Error{SNOG_ETIMEOUT, "job still has paths in flight"};
+        }
+      }
+    }
+    if (!req->error.empty()) throw Error{SNOG_EINVAL, req->error};
+    write_checkpoint(path, req->data);
+    return int(SNOG_OK);
+  });
+}
+
+int snog_server_submit_resume(SnogServer *server, uint32_t slot, const char *path, float *host_out,
+                              uint64_t *job_id) {
+  return api_call([&] {
+    if (!server || !path || !host_out || !job_id) throw Error{SNOG_EINVAL, "null argument"};
+    std::unique_ptr<Engine::Checkpoint> c(new Engine::Checkpoint(read_checkpoint(path)));
+    {
+      std::lock_guard<std::mutex> lk(server->mu);
+      if (!server->thread_error.empty()) throw Error{SNOG_ECUDA, "server stopped: " + server->thread_error};
+      const uint64_t id = server->next_id++;
+      server->inbox.push_back(SnogServer::Inbox{id, slot, c->cam, c->params, host_out, server->engine->now_ms()});
+      server->resumes[id] = std::move(c);
+      *job_id = id;
     }
     server->cv_work.notify_one();
     return int(SNOG_OK);

@@ -118,11 +118,24 @@ typedef struct SnogRenderParams {
   uint32_t spp;              /* [samples] */
   uint32_t min_path_len;     /* [surface_integ.min_path_len], default 3 */
   uint32_t max_path_len;     /* [surface_integ.max_path_len], default 25 */
-  uint32_t direct_samples;   /* [surface_integ.direct_samples], default 1 */
+  uint32_t direct_samples;   /* [surface_integ.direct_samples], default 1; with the
+                                direct integrator [surface_integ.light_samples],
+                                the reference's default 16 */
   float min_trace;           /* [min_trace], default 1e-3 */
   float bg_alpha;            /* [background_alpha], default 1 */
   uint64_t seed;             /* stream selector for the GPU's counter-based RNG */
+  uint32_t integrator;       /* [surface_integ.type]: SNOG_INTEG_PATH or SNOG_INTEG_DIRECT */
+  uint32_t reserved;         /* 0 */
 } SnogRenderParams;
+
+/* Surface integrators: PathInteg (render/path-integ.cc:134-407) and
+ * DirectInteg, direct lighting plus specular recursion with roulette beyond
+ * depth 5 (render/direct-integ.h:29-104, render/recursive-integ.cc:28-212).
+ * The direct integrator runs on the streaming engine (snog_render uses one
+ * internally); a surface that both reflects and transmits specularly starts
+ * a second ray, as the reference's recursion does.  min_path_len and
+ * max_path_len do not apply to it. */
+enum { SNOG_INTEG_PATH = 0, SNOG_INTEG_DIRECT = 1 };
 
 typedef struct SnogSceneInfo {
   uint32_t n_nodes, n_plist, max_depth, n_leaf_nodes;

@@ -353,6 +353,10 @@ struct RenderParams {
   float min_trace = 1e-3f;
   float background_alpha = 1.f;
   uint64_t seed = 0;
+  // [surface_integ.type]: "path" (SNOG_INTEG_PATH) or "direct"; the direct
+  // integrator takes its light samples per light from light_samples.
+  uint32_t integrator = SNOG_INTEG_PATH;
+  uint32_t light_samples = 16;
 };
 
 // The flattened scene uploaded to the device (Scene + Octree + light
@@ -599,7 +603,9 @@ class RenderMgr {
     p.spp = state_.params.samples;
     p.min_path_len = state_.params.min_path_len;
     p.max_path_len = state_.params.max_path_len;
-    p.direct_samples = state_.params.direct_samples;
+    p.integrator = state_.params.integrator;
+    p.direct_samples =
+        p.integrator == SNOG_INTEG_DIRECT ? state_.params.light_samples : state_.params.direct_samples;
     p.min_trace = state_.params.min_trace;
     p.bg_alpha = state_.params.background_alpha;
     p.seed = state_.params.seed;

@@ -209,10 +209,17 @@ void build_scene(RefScene &rs, const std::string &spec_path) {
   }
 
   rs.params.set("samples", unsigned(h.spp));
-  rs.params.set("surface_integ.type", std::string("path"));
-  rs.params.set("surface_integ.min_path_len", unsigned(h.min_path_len));
-  rs.params.set("surface_integ.max_path_len", unsigned(h.max_path_len));
-  rs.params.set("surface_integ.direct_samples", unsigned(h.direct_samples));
+  if (h.integrator == 1) {
+    // DirectInteg: direct lighting with light_samples per light, specular
+    // recursion (render/direct-integ.h:77-86)
+    rs.params.set("surface_integ.type", std::string("direct"));
+    rs.params.set("surface_integ.light_samples", unsigned(h.direct_samples));
+  } else {
+    rs.params.set("surface_integ.type", std::string("path"));
+    rs.params.set("surface_integ.min_path_len", unsigned(h.min_path_len));
+    rs.params.set("surface_integ.max_path_len", unsigned(h.max_path_len));
+    rs.params.set("surface_integ.direct_samples", unsigned(h.direct_samples));
+  }
   rs.params.set("min_trace", float(h.min_trace));
   rs.params.set("background_alpha", float(h.bg_alpha));
   rs.grs.reset(new GlobalRenderState(*rs.root, rs.params));

@@ -64,7 +64,9 @@ struct SpecHeader {
   float bg_alpha;                // [background_alpha]
   uint32_t has_normals;          // vertex normals follow the envmap (3 floats each)
   uint32_t right_handed;         // the mesh is right-handed (Mesh::left_handed false)
-  uint32_t reserved[6];
+  uint32_t integrator;           // [surface_integ.type]: 0 path, 1 direct (direct_samples
+                                 // is then [surface_integ.light_samples])
+  uint32_t reserved[5];
 };
 
 struct Scene {

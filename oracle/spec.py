@@ -72,9 +72,9 @@ def write_spec(path, scene, camera=None, params=None):
                      params.max_path_len, params.direct_samples], "<u4").tobytes()
     hdr += np.array([params.min_trace, params.bg_alpha], "<f4").tobytes()
     normals = getattr(scene, "normals", None)
-    hdr += np.array([1 if normals is not None else 0, 1 if getattr(scene, "right_handed", False) else 0],
-                    "<u4").tobytes()
-    hdr += np.zeros(6, "<u4").tobytes()
+    hdr += np.array([1 if normals is not None else 0, 1 if getattr(scene, "right_handed", False) else 0,
+                     getattr(params, "integrator", 0)], "<u4").tobytes()
+    hdr += np.zeros(5, "<u4").tobytes()
     with open(path, "wb") as f:
         f.write(hdr)
         f.write(np.ascontiguousarray(scene.materials).tobytes())

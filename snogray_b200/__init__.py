@@ -73,7 +73,7 @@ class SnogRenderParams(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
                 ("min_path_len", C.c_uint32), ("max_path_len", C.c_uint32),
                 ("direct_samples", C.c_uint32), ("min_trace", C.c_float), ("bg_alpha", C.c_float),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("integrator", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class SnogSceneInfo(C.Structure):
@@ -199,7 +199,7 @@ def camera_struct(cam: Camera) -> SnogCamera:
 
 def params_struct(p: RenderParams) -> SnogRenderParams:
     return SnogRenderParams(p.width, p.height, p.spp, p.min_path_len, p.max_path_len,
-                            p.direct_samples, p.min_trace, p.bg_alpha, p.seed)
+                            p.direct_samples, p.min_trace, p.bg_alpha, p.seed, p.integrator, 0)
 
 
 class Scene:

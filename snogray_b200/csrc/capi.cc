@@ -117,6 +117,7 @@ static void check_params(const SnogRenderParams &p) {
   if (p.width > 65536 || p.height > 65536) throw Error{SNOG_EINVAL, "image too large"};
   if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};
   if (p.direct_samples > 64) throw Error{SNOG_EINVAL, "direct_samples must be <= 64"};
+  if (p.integrator > SNOG_INTEG_DIRECT) throw Error{SNOG_EINVAL, "unknown integrator"};
   if (uint64_t(p.width + 4) * (p.height + 4) * p.spp >= (1ull << 40))
     throw Error{SNOG_EINVAL, "too many paths in one job"};
   if (uint64_t(p.width + 4) * (p.height + 4) >= (1ull << 32))
@@ -137,6 +138,10 @@ RenderPool &render_pool(int device) {
 static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
                         float *h_out, cudaStream_t st, SnogRenderStats *stats) {
   check_params(p);
+  if (p.integrator == SNOG_INTEG_DIRECT) {   // the streaming engine carries its spawned rays
+    render_on_engine(S, cam, p, d_out, h_out, st, stats);
+    return;
+  }
   if (!stack_class_for_depth(S.dev.max_depth))
     throw Error{SNOG_EINVAL, "octree deeper than the traversal kernels support (84 levels)"};
   RenderPool &pool = render_pool(S.device);

@@ -19,6 +19,11 @@ namespace snog {
 
 namespace {
 
+// Rays of the direct integrator go no deeper than the path state's 8-bit
+// length field; roulette beyond depth 5 makes that depth unreachable in
+// practice (survival 2^-249).
+constexpr uint32_t kMaxBounce = 255;
+
 struct EQ {                 // one ray queue, SoA of 16-byte records
   float4 *o, *d, *thr, *rad;
   uint4 *meta;              // x = path state, y = job, z/w = path index lo/hi
@@ -29,10 +34,21 @@ struct ESQ {                // shadow queue
   unsigned long long *tgt;  // address of the float4 radiance to add to
 };
 
-__global__ void k_e_plan(EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N, uint32_t cur) {
+__global__ void k_e_plan(EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N, uint32_t cur,
+                         uint32_t sp_cap) {
   const uint32_t n_cur = ctl->qcount[cur];
+  // Publish the branches the last shade spawned; the oldest waiting ones
+  // take free queue slots before new camera paths.
+  ctl->spawn_tail += ctl->spawn_n < ctl->spawn_room ? ctl->spawn_n : ctl->spawn_room;
+  const unsigned long long waiting = ctl->spawn_tail - ctl->spawn_head;
+  const uint32_t take = uint32_t(waiting < N - n_cur ? waiting : N - n_cur);
+  ctl->regen_spawn = take;
+  ctl->regen_spawn_head = ctl->spawn_head;
+  ctl->spawn_head += take;
+  ctl->spawn_n = 0;
+  ctl->spawn_room = sp_cap - uint32_t(ctl->spawn_tail - ctl->spawn_head);
   const unsigned long long avail = ctl->avail_end - ctl->ticket;
-  unsigned long long n_new = N - n_cur;
+  unsigned long long n_new = N - n_cur - take;
   if (n_new > avail) n_new = avail;
   // Retire items fully consumed before this iteration's tickets.
   unsigned long long head = ctl->item_head;
@@ -47,7 +63,7 @@ __global__ void k_e_plan(EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint3
   ctl->regen_base = n_cur;
   ctl->ticket += n_new;
   ctl->paths_started += n_new;
-  ctl->qcount[cur] = n_cur + uint32_t(n_new);
+  ctl->qcount[cur] = n_cur + take + uint32_t(n_new);
   ctl->qcount[cur ^ 1u] = 0;
   ctl->scount = 0;
   ctl->disp_closest = 0;
@@ -56,10 +72,20 @@ __global__ void k_e_plan(EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint3
 
 // New camera paths for tickets [regen_start, regen_start + regen_n).
 __global__ void __launch_bounds__(256) k_e_regen(EngineCtl *ctl, const WorkItem *ring, uint32_t R,
-                                                 const EngineJobDev *jobs, EQ q) {
-  const uint32_t n = ctl->regen_n;
+                                                 const EngineJobDev *jobs, EQ q, EQ sp, uint32_t sp_cap) {
+  const uint32_t n = ctl->regen_n, take = ctl->regen_spawn;
   const unsigned long long t0 = ctl->regen_start, head = ctl->item_head, tail = ctl->item_tail;
-  const uint32_t base = ctl->regen_base;
+  const unsigned long long sp_head = ctl->regen_spawn_head;
+  // Spawned branches first, into [base, base + take).
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < take; t += gridDim.x * blockDim.x) {
+    const uint32_t from = uint32_t((sp_head + t) % sp_cap), slot = ctl->regen_base + t;
+    q.o[slot] = sp.o[from];
+    q.d[slot] = sp.d[from];
+    q.thr[slot] = sp.thr[from];
+    q.rad[slot] = sp.rad[from];
+    q.meta[slot] = sp.meta[from];
+  }
+  const uint32_t base = ctl->regen_base + take;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const unsigned long long ticket = t0 + t;
     // Item holding this ticket: binary search over the ring window.
@@ -146,7 +172,8 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_shadow(
 __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
                                                  const DevScene *scenes, EQ qin, const uint32_t *hit_ref,
                                                  const float *hit_t, EQ qout, ESQ sq,
-                                                 unsigned long long *job_done) {
+                                                 unsigned long long *job_done, unsigned long long *job_spawned,
+                                                 EQ sp, uint32_t sp_cap) {
   const uint32_t n = ctl->qcount[cur];
   uint32_t *count_out = &ctl->qcount[cur ^ 1u];
   uint32_t *count_sq = &ctl->scount;
@@ -199,7 +226,10 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
       med = s->media[depth ? ps_medium(ps, depth - 1) : 0u];
       const float t1 = ref == PREF_END ? d4.w : t;
       thr = mul3(thr, medium_transmittance(med, length(xyz(d4)) * (t1 - o4.w)));
-      const bool include_emitters = bounce == 0 || ps_spec(ps) || jc.direct_samples == 0;
+      // The direct integrator adds every surface's own emission
+      // (RecursiveInteg::Lo, render/recursive-integ.cc:28-36).
+      const bool include_emitters =
+          jc.integ == SNOG_INTEG_DIRECT || bounce == 0 || ps_spec(ps) || jc.direct_samples == 0;
       if (ref == PREF_END) {
         if (include_emitters) rad = add(rad, mul3(background(*s, xyz(d4)), thr));
         if (bounce == 0 && rad.x == 0.f && rad.y == 0.f && rad.z == 0.f) alpha = jc.bg_alpha;
@@ -218,39 +248,100 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
     }
 
     // ---- continuation first, so shadow rays know where their path lives --
-    bool cont = false;
-    float3 thr_next = thr, next_d = f3(0, 0, 0);
+    // Path integrator: one BSDF sample over all lobes, roulette beyond
+    // min_path_len (render/path-integ.cc:309-385).  Direct integrator: the
+    // specular reflection and the specular transmission each continue with
+    // weight val |cos|, with roulette (survive 1/2 at weight 2) for rays
+    // deeper than 5 (render/recursive-integ.cc:28-116).  Both run through
+    // one bsdf_sample call site, so the BSDF code is inlined once.
+    bool cont = false, spawn = false;
+    float3 thr_next = thr, next_d = f3(0, 0, 0), thr_sp = f3(0, 0, 0), dir_sp = f3(0, 0, 0);
     float rr_next = rr_ratio;
-    uint32_t ps_next = ps;
+    uint32_t ps_next = ps, ps_sp = 0;
     if (alive) {
       const JobConsts &jc = J->jc;
-      const bool strat = bounce < jc.min_len;
-      float2 prm = strat ? strat_uv(strata_for(jc.S), rng, pixel, sidx, dim_of(bounce, K_BSDF))
-                         : rng.uv(dim_of(bounce, K_BSDF));
-      BSample bs = bsdf_sample(B, I, prm, B_ALL);
-      if (bs.pdf != 0.f && !(bs.val.x == 0.f && bs.val.y == 0.f && bs.val.z == 0.f)) {
-        thr_next = mul3(thr, mul(bs.val, fabsf(I.cos_n(bs.dir)) / bs.pdf));
-        bool stop = false;
-        if (bounce > jc.min_len) {
-          float p = fminf(intensity(thr_next) * rr_ratio, 1.f);
-          if (rng.u(dim_of(bounce, K_RR)) > p) {
-            stop = true;
-          } else {
-            thr_next = mul(thr_next, 1.f / p);
-            rr_next = rr_ratio * p;
-          }
+      const bool direct = jc.integ == SNOG_INTEG_DIRECT;
+      const uint32_t n_smp = direct ? 2u : 1u;
+      for (uint32_t k = 0; k < n_smp; k++) {
+        float2 prm = make_float2(0.f, 0.f);
+        uint32_t flags = B_SPECULAR | (k ? B_TRANSMISSIVE : B_REFLECTIVE);
+        if (!direct) {
+          prm = bounce < jc.min_len ? strat_uv(strata_for(jc.S), rng, pixel, sidx, dim_of(bounce, K_BSDF))
+                                    : rng.uv(dim_of(bounce, K_BSDF));
+          flags = B_ALL;
         }
-        if (!stop && bounce != jc.max_len) {
-          cont = true;
-          next_d = I.nf.from(bs.dir);
-          uint32_t nps = (ps & ~0x1ffu) | (bounce + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
-          if (bs.flags & B_TRANSMISSIVE) {
-            const uint32_t mid = s->mats[I.mat].medium_id;
-            if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
+        BSample bs = bsdf_sample(B, I, prm, flags);
+        float3 w;
+        bool go;
+        if (direct) {
+          go = csum(bs.val) > 0.f && bounce + 1u < kMaxBounce;
+          w = mul3(thr, mul(bs.val, fabsf(I.cos_n(bs.dir))));
+          if (go && bounce + 1u > 5u) {
+            if (rng.u(dim_of(bounce, K_RR) ^ (k << 20)) < 0.5f) go = false;
+            else w = mul(w, 2.f);
           }
+        } else {
+          go = bs.pdf != 0.f && !(bs.val.x == 0.f && bs.val.y == 0.f && bs.val.z == 0.f);
+          w = mul3(thr, mul(bs.val, fabsf(I.cos_n(bs.dir)) / bs.pdf));
+          if (go && bounce > jc.min_len) {
+            float p = fminf(intensity(w) * rr_ratio, 1.f);
+            if (rng.u(dim_of(bounce, K_RR)) > p) {
+              go = false;
+            } else {
+              w = mul(w, 1.f / p);
+              rr_next = rr_ratio * p;
+            }
+          }
+          go = go && bounce != jc.max_len;
+        }
+        if (!go) continue;
+        uint32_t nps = (ps & ~0x1ffu) | (bounce + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
+        if (bs.flags & B_TRANSMISSIVE) {
+          const uint32_t mid = s->mats[I.mat].medium_id;
+          if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
+        }
+        if (!cont) {
+          cont = true;
+          thr_next = w;
+          next_d = I.nf.from(bs.dir);
           ps_next = nps;
+        } else {
+          spawn = true;
+          thr_sp = w;
+          dir_sp = I.nf.from(bs.dir);
+          ps_sp = nps;
         }
       }
+    }
+    // A second ray waits in the spawn ring for a queue slot.  When the ring
+    // is full, one of the two rays continues, chosen with probability 1/2,
+    // at twice its weight -- an unbiased estimate of the pair's sum.
+    {
+      const uint32_t sslot = warp_append(&ctl->spawn_n, spawn);
+      if (spawn) {
+        if (sslot < ctl->spawn_room) {
+          const JobConsts &jc = J->jc;
+          const uint32_t at = uint32_t((ctl->spawn_tail + sslot) % sp_cap);
+          sp.o[at] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+          sp.d[at] = make_float4(dir_sp.x, dir_sp.y, dir_sp.z, jc.horizon);
+          sp.thr[at] = make_float4(thr_sp.x, thr_sp.y, thr_sp.z, 1.f);
+          sp.rad[at] = make_float4(0.f, 0.f, 0.f, 0.f);
+          sp.meta[at] = make_uint4(ps_sp, job, uint32_t(g), uint32_t(g >> 32));
+        } else {
+          if (rng.u(dim_of(bounce, K_RR) ^ (3u << 20)) < 0.5f) {
+            thr_next = thr_sp;
+            next_d = dir_sp;
+            ps_next = ps_sp;
+          }
+          thr_next = mul(thr_next, 2.f);
+          spawn = false;
+        }
+      }
+      // Spawned rays per job: a job is finished when its finished rays
+      // reach its paths plus its spawned rays.
+      const uint32_t key = spawn ? job : 0xffffffffu;
+      const unsigned m = __match_any_sync(0xffffffffu, key);
+      if (spawn && lane == uint32_t(__ffs(m) - 1)) atomicAdd(job_spawned + job, (unsigned long long)__popc(m));
     }
     const uint32_t slot = warp_append(count_out, cont);
     float4 *target = nullptr;
@@ -264,8 +355,17 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
         qout.meta[slot] = make_uint4(ps_next, job, uint32_t(g), uint32_t(g >> 32));
         target = qout.rad + slot;
       } else {
-        J->result[g] = make_float4(rad.x, rad.y, rad.z, alpha);
-        target = J->result + g;
+        float4 *res = J->result + g;
+        if (J->jc.integ == SNOG_INTEG_DIRECT) {
+          // several rays of one path end here: their radiance adds up
+          atomicAdd(&res->x, rad.x);
+          atomicAdd(&res->y, rad.y);
+          atomicAdd(&res->z, rad.z);
+          if (alpha != 0.f) atomicAdd(&res->w, alpha);
+        } else {
+          *res = make_float4(rad.x, rad.y, rad.z, alpha);
+        }
+        target = res;
       }
     }
     // Count finished paths per job, one atomic per group of lanes sharing a job.
@@ -298,7 +398,10 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
           const float inv_ns = 1.f / float(jc.direct_samples);
           const uint32_t kl = K_LIGHT0 + 3 * l;
           float2 pl, pb;
-          if (bounce < jc.min_len) {
+          // The direct integrator draws every depth's light samples from the
+          // pixel's stratified set, as its sample channels are shared down
+          // the recursion (render/recursive-integ.cc:28-36).
+          if (bounce < jc.min_len || jc.integ == SNOG_INTEG_DIRECT) {
             const Strata st_direct = strata_for(jc.S * jc.direct_samples);
             pl = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl));
             pb = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl + 1));
@@ -368,16 +471,17 @@ template <int STACK>
 void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N,
                       uint32_t cur, const EngineJobDev *jobs, const DevScene *scenes, EQ qc, EQ qn,
                       uint32_t *hit_ref, float *hit_t, ESQ sq, unsigned long long *job_done,
-                      const cudaEvent_t *ev) {
+                      unsigned long long *job_spawned, EQ sp, uint32_t sp_cap, const cudaEvent_t *ev) {
   const uint32_t sms = uint32_t(num_sms());
   if (ev) cudaEventRecord(ev[0], st);
-  k_e_plan<<<1, 1, 0, st>>>(ctl, ring, R, N, cur);
-  k_e_regen<<<sms * 8, 256, 0, st>>>(ctl, ring, R, jobs, qc);
+  k_e_plan<<<1, 1, 0, st>>>(ctl, ring, R, N, cur, sp_cap);
+  k_e_regen<<<sms * 8, 256, 0, st>>>(ctl, ring, R, jobs, qc, sp, sp_cap);
   if (ev) cudaEventRecord(ev[1], st);
   k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
                                                                                hit_t);
   if (ev) cudaEventRecord(ev[2], st);
-  k_e_shade<<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done);
+  k_e_shade<<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done, job_spawned,
+                                      sp, sp_cap);
   if (ev) cudaEventRecord(ev[3], st);
   k_e_shadow<STACK><<<resident_grid(k_e_shadow<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, scenes, sq);
   if (ev) cudaEventRecord(ev[4], st);
@@ -456,8 +560,13 @@ Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
   size_t o_href = take(4 * N), o_ht = take(4 * N);
   size_t o_so = take(16 * N * 2 * L), o_sd = take(16 * N * 2 * L), o_sc = take(16 * N * 2 * L),
          o_st = take(8 * N * 2 * L);
+  // Spawn ring for the direct integrator's second rays: a quarter of the
+  // queue (a full ring makes a vertex pick one of its two rays instead).
+  sp_cap_ = std::max<uint32_t>(cfg_.slots / 4, 1024);
+  size_t o_sp[5];
+  for (int a = 0; a < 5; a++) o_sp[a] = take(16 * size_t(sp_cap_));
   size_t o_ctl = take(sizeof(EngineCtl)), o_ring = take(sizeof(WorkItem) * cfg_.ring_items);
-  size_t o_jobs = take(sizeof(EngineJobDev) * cfg_.max_jobs), o_done = take(8 * size_t(cfg_.max_jobs));
+  size_t o_jobs = take(sizeof(EngineJobDev) * cfg_.max_jobs), o_done = take(16 * size_t(cfg_.max_jobs));
   size_t o_sc2 = take(sizeof(DevScene) * max_scenes_);
   check_cuda(cudaMalloc(&block_, off), "engine buffers");
   char *b = static_cast<char *>(block_);
@@ -468,6 +577,11 @@ Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
     q_rad_[k] = reinterpret_cast<float4 *>(b + o_q[k][3]);
     q_meta_[k] = reinterpret_cast<uint4 *>(b + o_q[k][4]);
   }
+  sp_o_ = reinterpret_cast<float4 *>(b + o_sp[0]);
+  sp_d_ = reinterpret_cast<float4 *>(b + o_sp[1]);
+  sp_thr_ = reinterpret_cast<float4 *>(b + o_sp[2]);
+  sp_rad_ = reinterpret_cast<float4 *>(b + o_sp[3]);
+  sp_meta_ = reinterpret_cast<uint4 *>(b + o_sp[4]);
   hit_ref_ = reinterpret_cast<uint32_t *>(b + o_href);
   hit_t_ = reinterpret_cast<float *>(b + o_ht);
   s_o_ = reinterpret_cast<float4 *>(b + o_so);
@@ -480,12 +594,12 @@ Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
   job_done_ = reinterpret_cast<unsigned long long *>(b + o_done);
   scenes_dev_ = reinterpret_cast<DevScene *>(b + o_sc2);
   check_cuda(cudaMemsetAsync(ctl_, 0, sizeof(EngineCtl), stream_), "memset");
-  check_cuda(cudaMemsetAsync(job_done_, 0, 8 * size_t(cfg_.max_jobs), stream_), "memset");
+  check_cuda(cudaMemsetAsync(job_done_, 0, 16 * size_t(cfg_.max_jobs), stream_), "memset");
   check_cuda(cudaMallocHost(&ctl_host_, sizeof(EngineCtl)), "pinned");
-  check_cuda(cudaMallocHost(&done_host_, 8 * size_t(cfg_.max_jobs)), "pinned");
+  check_cuda(cudaMallocHost(&done_host_, 16 * size_t(cfg_.max_jobs)), "pinned");
   staging_cap_ = size_t(cfg_.max_jobs) * sizeof(EngineJobDev) + size_t(cfg_.ring_items) * sizeof(WorkItem) + 4096;
   check_cuda(cudaMallocHost(&staging_, staging_cap_), "pinned staging");
-  std::memset(done_host_, 0, 8 * size_t(cfg_.max_jobs));
+  std::memset(done_host_, 0, 16 * size_t(cfg_.max_jobs));
   for (uint32_t k = cfg_.max_jobs; k > 0; k--) free_slots_.push_back(k - 1);
   check_cuda(cudaStreamSynchronize(stream_), "engine init");
 }
@@ -559,7 +673,8 @@ void Engine::launch_iterations() {
     const cudaEvent_t *ev = profile_on_ ? &events_[5 * it] : nullptr;
 #define SNOG_ITER(S)                                                                                          \
   launch_iteration<S>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], \
-                      q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_, ev)
+                      q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_, job_done_ + cfg_.max_jobs,            \
+                      EQ{sp_o_, sp_d_, sp_thr_, sp_rad_, sp_meta_}, sp_cap_, ev)
     switch (graph_stack_) {
       case 32: SNOG_ITER(32); break;
       case 64: SNOG_ITER(64); break;
@@ -594,6 +709,7 @@ uint64_t Engine::submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRe
   if (scene_slot >= scenes_.size()) throw Error{SNOG_ENOTFOUND, "unknown scene slot"};
   if (p.width == 0 || p.height == 0 || p.spp == 0) throw Error{SNOG_EINVAL, "width, height, spp must be > 0"};
   if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};
+  if (p.integrator > SNOG_INTEG_DIRECT) throw Error{SNOG_EINVAL, "unknown integrator"};
   if (p.direct_samples > 64) throw Error{SNOG_EINVAL, "direct_samples must be <= 64"};
   if (uint64_t(p.width + 4) * (p.height + 4) * p.spp >= (1ull << 32))
     throw Error{SNOG_EINVAL, "a job is limited to 2^32 paths"};
@@ -638,7 +754,7 @@ bool Engine::drained(uint64_t id) const {
   auto it = jobs_.find(id);
   if (it == jobs_.end()) return false;
   const HostJob &j = it->second;
-  return j.paused && j.table_slot != ~0u && done_host_[j.table_slot] >= j.pushed;
+  return j.paused && j.table_slot != ~0u && rays_done(j) >= j.pushed + rays_spawned(j);
 }
 
 void Engine::checkpoint(uint64_t id, Checkpoint &out) {
@@ -742,7 +858,12 @@ void Engine::admit() {
                                cudaMemcpyHostToDevice, stream_),
                "job record");
     check_cuda(cudaMemsetAsync(job_done_ + j.table_slot, 0, 8, stream_), "job counter");
+    check_cuda(cudaMemsetAsync(job_done_ + cfg_.max_jobs + j.table_slot, 0, 8, stream_), "job counter");
     done_host_[j.table_slot] = 0;
+    done_host_[cfg_.max_jobs + j.table_slot] = 0;
+    // The direct integrator's rays of one path add into its result.
+    if (j.jc.integ == SNOG_INTEG_DIRECT)
+      check_cuda(cudaMemsetAsync(j.result, 0, j.total * sizeof(float4), stream_), "result");
     if (j.resume) {
       // A resumed job: its finished paths come from the checkpoint and
       // count as done; work items start after them.
@@ -842,7 +963,8 @@ bool Engine::step() {
   }
   push_items();
   // After a launch (an even number of iterations) the live rays are in queue 0.
-  const bool inflight = last_ctl_.qcount[0] > 0 || last_ctl_.ticket < pushed_cum_;
+  const bool inflight = last_ctl_.qcount[0] > 0 || last_ctl_.ticket < pushed_cum_ ||
+                        last_ctl_.spawn_tail > last_ctl_.spawn_head || last_ctl_.spawn_n > 0;
   if (!inflight && active_.empty() && pending_.empty()) return false;
   // Launch while paths are in flight or an active job has work to push; a
   // job complete on the device is finished below either way.
@@ -854,7 +976,8 @@ bool Engine::step() {
   bool finishing = false;
   for (size_t k = 0; k < active_.size() && !finishing; k++) {
     const HostJob &j = jobs_.at(active_[k]);
-    finishing = done_host_[j.table_slot] >= j.total || (j.canceled && done_host_[j.table_slot] >= j.pushed);
+    finishing = rays_done(j) >= j.total + rays_spawned(j) ||
+                (j.canceled && rays_done(j) >= j.pushed + rays_spawned(j));
   }
   // Nothing to launch or finish: every remaining job is paused (or waits
   // for memory a paused job holds).  The caller waits for a command.
@@ -868,7 +991,7 @@ bool Engine::step() {
     }
     kernel_launches_ += 5 * 2 * cfg_.iters_per_launch;
     check_cuda(cudaMemcpyAsync(ctl_host_, ctl_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_), "ctl");
-    check_cuda(cudaMemcpyAsync(done_host_, job_done_, 8 * size_t(cfg_.max_jobs), cudaMemcpyDeviceToHost, stream_),
+    check_cuda(cudaMemcpyAsync(done_host_, job_done_, 16 * size_t(cfg_.max_jobs), cudaMemcpyDeviceToHost, stream_),
                "done");
     check_cuda(cudaStreamSynchronize(stream_), "iteration");
     staging_used_ = 0;
@@ -893,10 +1016,10 @@ bool Engine::step() {
   bool copies = false;
   for (size_t k = 0; k < active_.size(); k++) {
     HostJob &j = jobs_.at(active_[k]);
-    const uint64_t done = done_host_[j.table_slot];
-    if (done >= j.total || (j.canceled && done >= j.pushed)) {
+    const uint64_t done = rays_done(j), spawned = rays_spawned(j);
+    if (done >= j.total + spawned || (j.canceled && done >= j.pushed + spawned)) {
       done_idx.push_back(k);
-      if (done >= j.total && !j.cancel_sent) {   // complete before any cancel reached the device
+      if (done >= j.total + spawned && !j.cancel_sent) {   // complete before any cancel reached the device
         check_cuda(splat_job(j.jc, j.result, j.jit, j.total, j.accum, j.wsum, j.dev_out, stream_), "splat");
         kernel_launches_ += 2;
         if (!j.out_on_device)
@@ -910,7 +1033,7 @@ bool Engine::step() {
   for (size_t r = done_idx.size(); r-- > 0;) {
     const size_t k = done_idx[r];
     HostJob &j = jobs_.at(active_[k]);
-    j.st.status = (done_host_[j.table_slot] >= j.total && !j.cancel_sent) ? SNOG_OK : SNOG_ECANCELED;
+    j.st.status = (rays_done(j) >= j.total + rays_spawned(j) && !j.cancel_sent) ? SNOG_OK : SNOG_ECANCELED;
     j.st.finish_ms = t_fin;
     budget_used_ -= j.bytes;
     release_job(j);

@@ -68,6 +68,11 @@ struct EngineCtl {
   unsigned long long item_tail;    // one past the last pushed item (host-written)
   unsigned long long avail_end;    // cum + count of the last pushed item (host-written)
   unsigned long long rays_closest, rays_shadow, paths_started;
+  // Spawn ring: second specular rays of the direct integrator waiting for a
+  // queue slot.  Shade appends (spawn_n, up to spawn_room), plan publishes
+  // them and hands regen the oldest (regen_spawn from regen_spawn_head).
+  unsigned long long spawn_head, spawn_tail, regen_spawn_head;
+  uint32_t spawn_n, spawn_room, regen_spawn, pad_;
 };
 
 struct EngineConfigHost {
@@ -191,6 +196,10 @@ class Engine {
     JobStatsHost st;
   };
 
+  // Rays of job J finished / spawned as of the last step (a job is done
+  // when every path and every spawned ray has finished).
+  uint64_t rays_done(const HostJob &j) const { return done_host_[j.table_slot]; }
+  uint64_t rays_spawned(const HostJob &j) const { return done_host_[cfg_.max_jobs + j.table_slot]; }
   void build_graph();
   void launch_iterations();
   void admit();
@@ -217,7 +226,10 @@ class Engine {
   EngineCtl *ctl_;
   WorkItem *ring_;
   EngineJobDev *jobs_dev_;
-  unsigned long long *job_done_;
+  unsigned long long *job_done_;              // [max_jobs] finished rays, [max_jobs] spawned rays
+  float4 *sp_o_, *sp_d_, *sp_thr_, *sp_rad_;   // spawn ring, sp_cap_ entries
+  uint4 *sp_meta_;
+  uint32_t sp_cap_ = 0;
   DevScene *scenes_dev_;
   uint32_t max_scenes_ = 0;
   // host mirrors

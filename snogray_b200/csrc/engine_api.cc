@@ -31,6 +31,48 @@ extern thread_local std::string g_last_error;
 
 using namespace snog;
 
+namespace snog {
+
+void render_on_engine(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
+                      float *h_out, cudaStream_t st, SnogRenderStats *stats) {
+  static std::mutex mu;
+  static std::map<int, std::unique_ptr<Engine>> engines;
+  std::lock_guard<std::mutex> lk(mu);
+  // Queue sized so the shadow queue (two rays of 56 bytes per light sample
+  // per slot) stays near 2 GB.
+  const uint32_t ls = std::max(1u, S.dev.n_lights) * std::max(1u, p.direct_samples);
+  std::unique_ptr<Engine> &e = engines[S.device];
+  if (!e || e->config().max_lights < ls) {
+    e.reset();
+    EngineConfigHost c;
+    c.max_lights = std::max(4u, ls);
+    uint64_t slots = (2ull << 30) / (112ull * c.max_lights);
+    slots = std::min<uint64_t>(std::max<uint64_t>(slots, 1u << 16), 1u << 22);
+    c.slots = uint32_t(slots);
+    e.reset(new Engine(c));
+  }
+  check_cuda(cudaStreamSynchronize(st), "caller stream");   // the output buffer's earlier users
+  e->reset_scenes();
+  const uint32_t slot = e->add_scene(&S);
+  e->clear_counters();
+  const auto t0 = std::chrono::steady_clock::now();
+  const uint64_t id = e->submit(slot, cam, p, d_out ? d_out : h_out, d_out != nullptr);
+  e->run_to_completion();
+  const JobStatsHost js = e->stats(id);
+  if (js.status != SNOG_OK) throw Error{js.status, "render did not complete"};
+  if (stats) {
+    std::memset(stats, 0, sizeof *stats);
+    stats->paths = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
+    stats->closest_rays = e->rays_closest();
+    stats->shadow_rays = e->rays_shadow();
+    stats->device_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    stats->waves = 1;
+    stats->kernel_launches = e->launches();
+  }
+}
+
+}  // namespace snog
+
 namespace {
 
 template <class F>

@@ -115,6 +115,8 @@ extern "C" int snog_render_device_noalloc(SnogScene *scene, const SnogCamera *ca
     SceneImpl &S = *scene->impl;
     if (!S.on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
     const SnogRenderParams &p = *params;
+    if (p.integrator != SNOG_INTEG_PATH)
+      throw Error{SNOG_EINVAL, "the no-alloc render runs the path integrator only"};
     if (p.width == 0 || p.height == 0 || p.spp == 0)
       throw Error{SNOG_EINVAL, "width, height and spp must be positive"};
     if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};

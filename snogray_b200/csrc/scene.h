@@ -75,6 +75,12 @@ SceneImpl *build_scene(const SnogSceneDesc &desc, bool upload = true, uint32_t o
 // tree.
 const OctreeArrays &host_octree(SceneImpl &S);
 
+// One job rendered on a streaming engine kept per device (engine_api.cc):
+// the plain render calls use it for the direct integrator.  Synchronous;
+// D_OUT (device) or H_OUT (host) receives the image.
+void render_on_engine(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
+                      float *h_out, cudaStream_t st, SnogRenderStats *stats);
+
 struct Error {
   int code;
   std::string msg;

@@ -201,6 +201,7 @@ __device__ __forceinline__ float4 *ring_slots() {
 
 constexpr uint32_t kGateFlag = 8u;   // entry carries a parent gate
 constexpr uint32_t kSlowSlab = 8u;   // in Traversal::octant: slab bounds may be NaN
+constexpr uint32_t kAnyHit = 16u;    // in Traversal::octant: an any-hit query
 
 __device__ __forceinline__ bool slab_open(float t0, float t1, float3 lo, float3 hi) {
   float min_t = fmax_ref(t0, fmax_ref(lo.x, fmax_ref(lo.y, lo.z)));
@@ -244,7 +245,7 @@ template <int STACK>
 struct Traversal {
   float3 o, d, lo, hi;
   float t0, t1;
-  uint32_t node, gate, octant, hit_ref;   // octant: bits 0-2, kSlowSlab
+  uint32_t node, gate, octant, hit_ref;   // octant: bits 0-2, kSlowSlab, kAnyHit
   uint32_t lp, lend;         // surface list still to test: plist[lp, lend)
   uint32_t ring;             // shared-memory ring: oldest position | count << 4 (0 when empty)
   int sp;                    // entries spilled to stk[0, sp)
@@ -364,12 +365,19 @@ struct Traversal {
     have = false;
     const bool slow = !FAST || (octant & kSlowSlab);
     bool open = true;
-    if (gate & kGateFlag) open = gate_open(gate & 7u, t0, t1, lo, hi);
-    if (open) {
+    if ((gate & kGateFlag) && (octant & kAnyHit)) {
+      // An any-hit query's extent never changes, so an entry with a parent
+      // gate passed the very gate and cull it would be given now when it
+      // was pushed (or entered): the call happens and the node is open.
       cnt.nodes++;
-      open = slow ? slab_open(t0, t1, lo, hi) : slab_open_finite(t0, t1, lo, hi);
+    } else {
+      if (gate & kGateFlag) open = gate_open(gate & 7u, t0, t1, lo, hi);
+      if (open) {
+        cnt.nodes++;
+        open = slow ? slab_open(t0, t1, lo, hi) : slab_open_finite(t0, t1, lo, hi);
+      }
+      if (!open) return;
     }
-    if (!open) return;
     const uint4 nd = __ldg(nodes + node);
     lp = nd.z;
     lend = nd.z + nd.w;
@@ -606,6 +614,7 @@ __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, Trac
     if (got != RayDispenser::kIdle) {
       ray = got;
       start(ray, tr, any);
+      if (any) tr.octant |= kAnyHit;
     }
     const bool busy = ray != RayDispenser::kIdle;
     // Visit nodes only while the warp's pending list entries would not fill

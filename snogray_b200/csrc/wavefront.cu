@@ -594,6 +594,7 @@ JobConsts make_job(const DevScene &s, const SnogCamera &cam, const SnogRenderPar
   jc.tan_y = cam.tan_half_fov_y;
   jc.seed_lo = uint32_t(p.seed) * 2654435761u + 0x1234567u;
   jc.seed_hi = uint32_t(p.seed >> 32) ^ 0x9e3779b9u;
+  jc.integ = p.integrator;
   return jc;
 }
 

@@ -23,6 +23,7 @@ struct JobConsts {
   float tan_x, tan_y;
   uint32_t u_steps, v_steps, cells;
   uint32_t seed_lo, seed_hi;
+  uint32_t integ;           // SNOG_INTEG_PATH or SNOG_INTEG_DIRECT
 };
 
 // Device buffers for one wave of paths (sized for wave_cap paths).

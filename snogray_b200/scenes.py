@@ -122,6 +122,8 @@ class RenderParams:
     min_trace: float = 1e-3            # min_trace
     bg_alpha: float = 1.0              # background_alpha
     seed: int = 0
+    integrator: int = 0                # surface_integ.type: 0 path, 1 direct (direct_samples =
+                                       # surface_integ.light_samples)
 
 
 def material(mtype, color=(0, 0, 0), gloss=(1, 1, 1), m=0.0, ior_n=1.5, ior_k=0.0,
@@ -181,6 +183,13 @@ def cornell_camera(width, height):
 def cornell_params(width=256, height=256, spp=16, seed=0):
     return RenderParams(width=width, height=height, spp=spp, min_path_len=3, max_path_len=8,
                         direct_samples=1, seed=seed)
+
+
+def direct_params(width=128, height=128, spp=16, seed=0, light_samples=4):
+    """The direct-lighting integrator (surface_integ.type = direct) with
+    LIGHT_SAMPLES samples per light."""
+    return RenderParams(width=width, height=height, spp=spp, direct_samples=light_samples, integrator=1,
+                        seed=seed)
 
 
 # ---------------------------------------------------------------------------

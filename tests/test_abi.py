@@ -28,7 +28,7 @@ def test_every_declared_symbol_is_exported():
 def test_header_structs_match_ctypes_layout():
     # Sizes the Python binding assumes for the C structs.
     assert ctypes.sizeof(sb.SnogCamera) == 14 * 4
-    assert ctypes.sizeof(sb.SnogRenderParams) == 8 * 4 + 8
+    assert ctypes.sizeof(sb.SnogRenderParams) == 8 * 4 + 8 + 2 * 4
     assert scenes.MAT_DTYPE.itemsize == 4 * 14
     assert scenes.SPHERE_DTYPE.itemsize == 20
     assert scenes.TRIPAR_DTYPE.itemsize == 44

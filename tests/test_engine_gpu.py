@@ -158,3 +158,41 @@ def test_many_scenes_in_one_batch():
     for (sc, cam, p), img in zip(jobs, imgs):
         ref, _ = sc.render(cam, p)
         assert np.allclose(img, ref, rtol=RTOL, atol=ATOL)
+
+
+def test_direct_integrator_spawn_ring_overflow_is_unbiased(golden):
+    """The direct integrator starts a second ray where glass both reflects and
+    transmits; with a tiny queue the spawn ring is full most of the time and
+    vertices keep one of their two rays at twice the weight.  Image means stay
+    within 3 standard errors of the reference's (render_cornell_direct)."""
+    import math
+    g = golden("render_cornell_direct.npz")
+    w, h, spp = int(g["width"]), int(g["height"]), int(g["spp"])
+    cfg = sb.engine_config(slots=4096, item_paths=1024, ring_items=256)
+    means = []
+    with sb.Scene(scenes.cornell_box()) as sc:
+        cam = scenes.cornell_camera(w, h)
+        for k in range(32):
+            imgs, st = sb.render_batch([(sc, cam, scenes.direct_params(w, h, spp, seed=100 + k))], config=cfg)
+            means.append(imgs[0].reshape(-1, 3).mean(0))
+    means = np.array(means)
+    m = means.mean(0)
+    se = np.sqrt((means.std(0, ddof=1) / math.sqrt(len(means))) ** 2 + g["se"] ** 2)
+    z = np.abs(m - g["mean"]) / se
+    assert (z < 3).all(), f"means {m} ref {g['mean']} z {z}"
+
+
+def test_direct_integrator_same_through_plain_batch_and_server():
+    sd = scenes.cornell_box()
+    cam = scenes.cornell_camera(40, 32)
+    p = scenes.direct_params(40, 32, 8, seed=5)
+    with sb.Scene(sd) as sc:
+        plain, st = sc.render(cam, p)
+        batch, _ = sb.render_batch([(sc, cam, p)])
+        with sb.Server() as srv:
+            served, sst = srv.wait(srv.submit(srv.add_scene(sc), cam, p))
+    assert st["paths"] == 44 * 36 * 8 and st["shadow_rays"] > 0
+    assert np.isfinite(plain).all() and plain.mean() > 0.05
+    for img in (batch[0], served):
+        assert np.allclose(img, plain, rtol=1e-5, atol=1e-6), np.abs(img - plain).max()
+

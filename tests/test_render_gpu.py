@@ -39,7 +39,7 @@ def _render_k(name, k, seed0=1):
 @pytest.mark.parametrize("name", sorted(RENDER_CASES))
 def test_image_mean_within_3se(name, golden):
     g = golden(f"render_{name}.npz")
-    sd, imgs, st = _render_k(name, K_GPU)
+    sd, imgs, st = _render_k(name, max(K_GPU, int(g["k"])))
     assert scenes.scene_digest(sd) == str(g["scene_digest"])
     assert imgs.shape[1:] == (int(g["height"]), int(g["width"]), 3)
     assert np.isfinite(imgs).all() and (imgs >= 0).all()
@@ -54,7 +54,7 @@ def test_image_mean_within_3se(name, golden):
 @pytest.mark.parametrize("name", sorted(RENDER_CASES))
 def test_rmse_vs_ground_truth(name, golden):
     g = golden(f"render_{name}.npz")
-    _, imgs, _ = _render_k(name, K_GPU, seed0=1000)
+    _, imgs, _ = _render_k(name, max(K_GPU, int(g["k"])), seed0=100000)
     gt = g["gt"].astype(np.float32)
     rmse = np.sqrt(((imgs - gt[None]) ** 2).reshape(len(imgs), -1).mean(1))
     gpu, cpu = float(np.median(rmse)), float(np.median(g["rmse"]))

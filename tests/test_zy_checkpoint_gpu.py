@@ -9,6 +9,7 @@ agree up to the order of those additions (rtol 1e-5, as in the renderer's
 determinism test).  Paused jobs free the device for other jobs.
 """
 
+import ctypes
 import os
 import time
 
@@ -20,7 +21,7 @@ from snogray_b200 import scenes
 
 pytestmark = pytest.mark.gpu
 
-CKP_HEAD = 8 + 56 + 40          # magic, SnogCamera, SnogRenderParams
+CKP_HEAD = 8 + ctypes.sizeof(sb.SnogCamera) + ctypes.sizeof(sb.SnogRenderParams)   # magic, camera, params
 
 
 def _job(w=1024, h=1024, spp=64, seed=9):

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_closest
   const uint32_t n = ctl->qcount[cur];
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_closest += n;
   TraceCounters c{0, 0, 0};
-  trace_loop<STACK>(
+  trace_loop<STACK, kClosestOnly>(
       &ctl->disp_closest, n, c,
       [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
         const float4 o = q.o[ray], d = q.d[ray];
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_shadow(
   const uint32_t n = ctl->scount;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_shadow += n;
   TraceCounters c{0, 0, 0};
-  trace_loop<STACK>(
+  trace_loop<STACK, kAnyOnly>(
       &ctl->disp_shadow, n, c,
       [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
         const float4 o = q.o[ray], d = q.d[ray];
@@ -169,6 +169,9 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_shadow(
 // stalls on instruction fetch, and more resident warps hide that better than
 // the spill-free 117-register build at 4 blocks (measured 104 -> 88 ms per
 // terrain frame).
+// DIRECT: the direct integrator's code is compiled in (launched while a job
+// of that integrator is active; the path integrator's kernel stays smaller).
+template <bool DIRECT>
 __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
                                                  const DevScene *scenes, EQ qin, const uint32_t *hit_ref,
                                                  const float *hit_t, EQ qout, ESQ sq,
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
       // The direct integrator adds every surface's own emission
       // (RecursiveInteg::Lo, render/recursive-integ.cc:28-36).
       const bool include_emitters =
-          jc.integ == SNOG_INTEG_DIRECT || bounce == 0 || ps_spec(ps) || jc.direct_samples == 0;
+          (DIRECT && jc.integ == SNOG_INTEG_DIRECT) || bounce == 0 || ps_spec(ps) || jc.direct_samples == 0;
       if (ref == PREF_END) {
         if (include_emitters) rad = add(rad, mul3(background(*s, xyz(d4)), thr));
         if (bounce == 0 && rad.x == 0.f && rad.y == 0.f && rad.z == 0.f) alpha = jc.bg_alpha;
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
     uint32_t ps_next = ps, ps_sp = 0;
     if (alive) {
       const JobConsts &jc = J->jc;
-      const bool direct = jc.integ == SNOG_INTEG_DIRECT;
+      const bool direct = (DIRECT && jc.integ == SNOG_INTEG_DIRECT);
       const uint32_t n_smp = direct ? 2u : 1u;
       for (uint32_t k = 0; k < n_smp; k++) {
         float2 prm = make_float2(0.f, 0.f);
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
         target = qout.rad + slot;
       } else {
         float4 *res = J->result + g;
-        if (J->jc.integ == SNOG_INTEG_DIRECT) {
+        if (DIRECT && J->jc.integ == SNOG_INTEG_DIRECT) {
           // several rays of one path end here: their radiance adds up
           atomicAdd(&res->x, rad.x);
           atomicAdd(&res->y, rad.y);
@@ -401,7 +404,7 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
           // The direct integrator draws every depth's light samples from the
           // pixel's stratified set, as its sample channels are shared down
           // the recursion (render/recursive-integ.cc:28-36).
-          if (bounce < jc.min_len || jc.integ == SNOG_INTEG_DIRECT) {
+          if (bounce < jc.min_len || (DIRECT && jc.integ == SNOG_INTEG_DIRECT)) {
             const Strata st_direct = strata_for(jc.S * jc.direct_samples);
             pl = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl));
             pb = strat_uv(st_direct, rng, pixel, sidx * jc.direct_samples + jn, dim_of(bounce, kl + 1));
@@ -471,7 +474,8 @@ template <int STACK>
 void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N,
                       uint32_t cur, const EngineJobDev *jobs, const DevScene *scenes, EQ qc, EQ qn,
                       uint32_t *hit_ref, float *hit_t, ESQ sq, unsigned long long *job_done,
-                      unsigned long long *job_spawned, EQ sp, uint32_t sp_cap, const cudaEvent_t *ev) {
+                      unsigned long long *job_spawned, EQ sp, uint32_t sp_cap, bool direct,
+                      const cudaEvent_t *ev) {
   const uint32_t sms = uint32_t(num_sms());
   if (ev) cudaEventRecord(ev[0], st);
   k_e_plan<<<1, 1, 0, st>>>(ctl, ring, R, N, cur, sp_cap);
@@ -480,8 +484,12 @@ void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uin
   k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
                                                                                hit_t);
   if (ev) cudaEventRecord(ev[2], st);
-  k_e_shade<<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done, job_spawned,
-                                      sp, sp_cap);
+  if (direct)
+    k_e_shade<true><<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done,
+                                              job_spawned, sp, sp_cap);
+  else
+    k_e_shade<false><<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done,
+                                               job_spawned, sp, sp_cap);
   if (ev) cudaEventRecord(ev[3], st);
   k_e_shadow<STACK><<<resident_grid(k_e_shadow<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, scenes, sq);
   if (ev) cudaEventRecord(ev[4], st);
@@ -607,7 +615,8 @@ Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto &kv : jobs_) release_job(kv.second);
-  if (graph_) cudaGraphExecDestroy(graph_);
+  for (cudaGraphExec_t &gx : graph_)
+    if (gx) cudaGraphExecDestroy(gx);
   cache_.trim();
   cudaFree(block_);
   cudaFreeHost(ctl_host_);
@@ -647,8 +656,10 @@ uint32_t Engine::add_scene(SceneImpl *scene) {
   check_cuda(cudaStreamSynchronize(stream_), "scene table");
   const int sc = stack_class_for_depth(scene->dev.max_depth);
   if (sc > graph_stack_) {
-    if (graph_) cudaGraphExecDestroy(graph_);
-    graph_ = nullptr;
+    for (cudaGraphExec_t &gx : graph_) {
+      if (gx) cudaGraphExecDestroy(gx);
+      gx = nullptr;
+    }
     graph_stack_ = sc;
   }
   return slot;
@@ -656,7 +667,7 @@ uint32_t Engine::add_scene(SceneImpl *scene) {
 
 // Every iteration of one launch (iters_per_launch pairs, queue 0 -> 1 -> 0),
 // with events around the kernels while profiling.
-void Engine::launch_iterations() {
+void Engine::launch_iterations(bool direct) {
   EQ q[2];
   for (int k = 0; k < 2; k++) q[k] = EQ{q_o_[k], q_d_[k], q_thr_[k], q_rad_[k], q_meta_[k]};
   ESQ sq{s_o_, s_d_, s_c_, s_tgt_};
@@ -674,7 +685,7 @@ void Engine::launch_iterations() {
 #define SNOG_ITER(S)                                                                                          \
   launch_iteration<S>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], \
                       q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_, job_done_ + cfg_.max_jobs,            \
-                      EQ{sp_o_, sp_d_, sp_thr_, sp_rad_, sp_meta_}, sp_cap_, ev)
+                      EQ{sp_o_, sp_d_, sp_thr_, sp_rad_, sp_meta_}, sp_cap_, direct, ev)
     switch (graph_stack_) {
       case 32: SNOG_ITER(32); break;
       case 64: SNOG_ITER(64); break;
@@ -685,16 +696,16 @@ void Engine::launch_iterations() {
   }
 }
 
-void Engine::build_graph() {
+void Engine::build_graph(bool direct) {
   cudaGraph_t g;
   const bool prof = profile_on_;
   profile_on_ = false;
   check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
-  launch_iterations();
+  launch_iterations(direct);
   profile_on_ = prof;
   cudaError_t e = cudaStreamEndCapture(stream_, &g);
   check_cuda(e, "end capture");
-  e = cudaGraphInstantiate(&graph_, g, 0);
+  e = cudaGraphInstantiate(&graph_[direct], g, 0);
   cudaGraphDestroy(g);
   check_cuda(e, "graph instantiate");
 }
@@ -982,12 +993,17 @@ bool Engine::step() {
   // Nothing to launch or finish: every remaining job is paused (or waits
   // for memory a paused job holds).  The caller waits for a command.
   if (!work && !finishing) return false;
+  // The shading kernel with the direct integrator's code while a job of that
+  // integrator is active (spawned rays belong to such jobs).
+  bool direct = false;
+  for (size_t k = 0; k < active_.size() && !direct; k++)
+    direct = jobs_.at(active_[k]).jc.integ == SNOG_INTEG_DIRECT;
   if (work) {
     if (profile_on_) {
-      launch_iterations();
+      launch_iterations(direct);
     } else {
-      if (!graph_) build_graph();
-      check_cuda(cudaGraphLaunch(graph_, stream_), "graph launch");
+      if (!graph_[direct]) build_graph(direct);
+      check_cuda(cudaGraphLaunch(graph_[direct], stream_), "graph launch");
     }
     kernel_launches_ += 5 * 2 * cfg_.iters_per_launch;
     check_cuda(cudaMemcpyAsync(ctl_host_, ctl_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_), "ctl");

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_BATCH_MINBLOCKS) k_tra
         const PrimRec r = load_prim(s, ref);
         if (r.a.w == float(PRIM_SPHERE)) {
           // Sphere::IsecInfo::normal: (ray.end () - centre).unit () (surface/sphere.cc:96-100)
-          float3 end = xadd(tr.o, xmul(tr.d, tr.t1));
+          float3 end = xadd(tr.ray_o(), xmul(tr.ray_d(), tr.t1));
           float3 v = xsub(end, xyz(r.a));
           nv = xmul(v, __fdiv_rn(1.0f, __fsqrt_rn(xlen_sq(v))));
         } else {

@@ -199,9 +199,19 @@ __device__ __forceinline__ float4 *ring_slots() {
   return ring + threadIdx.x;
 }
 
+// Each thread's current ray in shared memory, for the lanes that test its
+// list entries (a list round would otherwise move 14 values by shuffles):
+// uint4 k * kTraceBlock + threadIdx.x holds, for k = 0, 1, 2, (origin, t0),
+// (direction, t1) and the scene's list and primitive pointers.
+__device__ __forceinline__ uint4 *ray_slots() {
+  __shared__ uint4 rays[3 * kTraceBlock];
+  return rays;
+}
+
 constexpr uint32_t kGateFlag = 8u;   // entry carries a parent gate
 constexpr uint32_t kSlowSlab = 8u;   // in Traversal::octant: slab bounds may be NaN
 constexpr uint32_t kAnyHit = 16u;    // in Traversal::octant: an any-hit query
+enum { kClosestOnly = 0, kAnyOnly = 1, kMixed = 2 };   // queries a trace kernel runs
 
 __device__ __forceinline__ bool slab_open(float t0, float t1, float3 lo, float3 hi) {
   float min_t = fmax_ref(t0, fmax_ref(lo.x, fmax_ref(lo.y, lo.z)));
@@ -243,21 +253,32 @@ __device__ __forceinline__ uint32_t visit_bits(uint32_t i) { return i == 3u ? 4u
 // cnt.overflow is set and the result must be discarded.
 template <int STACK>
 struct Traversal {
-  float3 o, d, lo, hi;
+  float3 lo, hi;
   float t0, t1;
   uint32_t node, gate, octant, hit_ref;   // octant: bits 0-2, kSlowSlab, kAnyHit
   uint32_t lp, lend;         // surface list still to test: plist[lp, lend)
   uint32_t ring;             // shared-memory ring: oldest position | count << 4 (0 when empty)
   int sp;                    // entries spilled to stk[0, sp)
   bool have;                 // a current entry (node/gate/lo/hi) is set
-  const uint4 *nodes;        // the ray's scene
-  const uint32_t *plist;
-  const float4 *prims;
+  const uint4 *nodes;        // the ray's scene (its list and primitive arrays are in the ray slot)
   StackEntry stk[STACK];
 
-  __device__ __forceinline__ void init(const DevScene &s, float3 o_, float3 d_, float t0_, float t1_) {
-    o = o_;
-    d = d_;
+  // The ray's origin and direction, from its shared-memory slot.
+  __device__ __forceinline__ float3 ray_o() const {
+    const uint4 a = ray_slots()[threadIdx.x];
+    return f3(__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z));
+  }
+  __device__ __forceinline__ float3 ray_d() const {
+    const uint4 a = ray_slots()[kTraceBlock + threadIdx.x];
+    return f3(__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z));
+  }
+  // Shrink the ray (closest queries), in the register and in the slot.
+  __device__ __forceinline__ void set_t1(float t) {
+    t1 = t;
+    reinterpret_cast<uint32_t *>(ray_slots() + kTraceBlock + threadIdx.x)[3] = __float_as_uint(t);
+  }
+
+  __device__ __forceinline__ void init(const DevScene &s, float3 o, float3 d, float t0_, float t1_) {
     t0 = t0_;
     t1 = t1_;
     hit_ref = PREF_END;
@@ -268,8 +289,14 @@ struct Traversal {
     lp = lend = 0;
     have = s.n_nodes != 0;
     nodes = s.nodes;
-    plist = s.plist;
-    prims = s.prims;
+    {
+      uint4 *slot = ray_slots() + threadIdx.x;
+      const unsigned long long pl = reinterpret_cast<uintptr_t>(s.plist), pr = reinterpret_cast<uintptr_t>(s.prims);
+      slot[0] = make_uint4(__float_as_uint(o.x), __float_as_uint(o.y), __float_as_uint(o.z), __float_as_uint(t0_));
+      slot[kTraceBlock] =
+          make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z), __float_as_uint(t1_));
+      slot[2 * kTraceBlock] = make_uint4(uint32_t(pl), uint32_t(pl >> 32), uint32_t(pr), uint32_t(pr >> 32));
+    }
     // 1 / d rounded once, as the reference's division (__frcp_rn is the
     // correctly rounded reciprocal, the same value as 1.0f / d).
     float inv = (d.x == 0.f) ? 1e9f : __frcp_rn(d.x);
@@ -359,13 +386,16 @@ struct Traversal {
   // tests, which only admits more children (the ray can only shrink), and
   // every entry's gate and cull are evaluated again when it is entered -- so
   // the tests and their order are the reference's.
-  template <bool FAST = true>
+  // ANY: the queries the calling kernel runs -- kClosestOnly, kAnyOnly or
+  // kMixed (checked per ray) -- so closest-hit kernels carry no any-hit branch.
+  template <bool FAST = true, int ANY = kMixed>
   __device__ __forceinline__ void node_step(TraceCounters &cnt) {
     if (!have && !pop()) return;
     have = false;
     const bool slow = !FAST || (octant & kSlowSlab);
     bool open = true;
-    if ((gate & kGateFlag) && (octant & kAnyHit)) {
+    const bool any_query = ANY == kAnyOnly || (ANY == kMixed && (octant & kAnyHit));
+    if ((gate & kGateFlag) && any_query) {
       // An any-hit query's extent never changes, so an entry with a parent
       // gate passed the very gate and cull it would be given now when it
       // was pushed (or entered): the call happens and the node is open.
@@ -486,6 +516,7 @@ template <int STACK>
 __device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool any, TraceCounters &cnt) {
   constexpr unsigned kFull = 0xffffffffu;
   const uint32_t lane = threadIdx.x & 31u;
+  __syncwarp();   // the warp's ray-slot writes (new rays, shrunk t1) are visible
   uint32_t c = want ? tr.lend - tr.lp : 0u;
   c = c < 32u ? c : 32u;
   uint32_t incl = c;
@@ -506,21 +537,20 @@ __device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool
   // The owner's ray and list.
   const uint32_t o_excl = __shfl_sync(kFull, excl, own);
   const uint32_t o_lp = __shfl_sync(kFull, tr.lp, own);
-  const unsigned long long o_plist =
-      __shfl_sync(kFull, (unsigned long long)reinterpret_cast<uintptr_t>(tr.plist), own);
-  const unsigned long long o_prims =
-      __shfl_sync(kFull, (unsigned long long)reinterpret_cast<uintptr_t>(tr.prims), own);
-  const float3 ro = f3(__shfl_sync(kFull, tr.o.x, own), __shfl_sync(kFull, tr.o.y, own),
-                       __shfl_sync(kFull, tr.o.z, own));
-  const float3 rd = f3(__shfl_sync(kFull, tr.d.x, own), __shfl_sync(kFull, tr.d.y, own),
-                       __shfl_sync(kFull, tr.d.z, own));
-  const float rt0 = __shfl_sync(kFull, tr.t0, own);
-  const float rt1 = __shfl_sync(kFull, tr.t1, own);
   const bool o_any = (__ballot_sync(kFull, any) >> own) & 1u;
   uint32_t pid = PREF_END;
   bool hit = false;
-  float th = rt1;
+  float th = 0.f;
   if (item) {
+    const uint4 *slot = ray_slots() + ((threadIdx.x & ~31u) + own);
+    const uint4 ra = slot[0], rb = slot[kTraceBlock];
+    const float3 ro = f3(__uint_as_float(ra.x), __uint_as_float(ra.y), __uint_as_float(ra.z));
+    const float3 rd = f3(__uint_as_float(rb.x), __uint_as_float(rb.y), __uint_as_float(rb.z));
+    const float rt0 = __uint_as_float(ra.w);
+    th = __uint_as_float(rb.w);
+    const uint4 rc = slot[2 * kTraceBlock];
+    const unsigned long long o_plist = (unsigned long long)rc.x | ((unsigned long long)rc.y << 32);
+    const unsigned long long o_prims = (unsigned long long)rc.z | ((unsigned long long)rc.w << 32);
     pid = __ldg(reinterpret_cast<const uint32_t *>(o_plist) + o_lp + (lane - o_excl));
     const float4 *p = reinterpret_cast<const float4 *>(o_prims) + 3 * size_t(pid);
     const PrimRec r{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
@@ -545,7 +575,7 @@ __device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool
       tr.lp = tr.lend;
       return true;
     }
-    tr.t1 = b_t;
+    tr.set_t1(b_t);
   }
   cnt.tests += used;
   tr.lp += used;
@@ -599,7 +629,7 @@ struct RayDispenser {
 // round of list entries pending, every live lane without a list pending
 // visits one octree entry; then the warp tests one round of pending list
 // entries together.  All 32 lanes of every warp must run it.
-template <int STACK, bool FAST = true, class Start, class Done>
+template <int STACK, int ANY = kMixed, class Start, class Done>
 __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, TraceCounters &cnt, Start start,
                                            Done done) {
   Traversal<STACK> tr;
@@ -621,7 +651,7 @@ __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, Trac
     // a round: list rounds run full, node steps run with more lanes at once.
     const uint32_t pend = (busy && tr.lp < tr.lend) ? tr.lend - tr.lp : 0u;
     const uint32_t pending = __reduce_add_sync(0xffffffffu, pend < 32u ? pend : 32u);
-    if (pending < 32u && busy && tr.lp >= tr.lend && !tr.finished()) tr.template node_step<FAST>(cnt);
+    if (pending < 32u && busy && tr.lp >= tr.lend && !tr.finished()) tr.template node_step<true, ANY>(cnt);
     const bool stop = list_round(tr, busy && tr.lp < tr.lend, any, cnt);
     if (busy && (stop || tr.finished())) {
       done(ray, tr, any);

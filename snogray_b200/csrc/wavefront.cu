@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_clo
     stats[0] += n;
   }
   TraceCounters c{0, 0, 0};
-  trace_loop<STACK>(
+  trace_loop<STACK, kClosestOnly>(
       counters + 4, n, c,
       [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
         const float4 o = q.o[ray], d = q.d[ray];
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_sha
   const uint32_t n = counters[2];
   if (blockIdx.x == 0 && threadIdx.x == 0) stats[1] += n;
   TraceCounters c{0, 0, 0};
-  trace_loop<STACK>(
+  trace_loop<STACK, kAnyOnly>(
       counters + 5, n, c,
       [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
         const float4 o = q.o[ray], d = q.d[ray];

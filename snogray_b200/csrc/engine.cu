@@ -34,6 +34,11 @@ struct ESQ {                // shadow queue
   unsigned long long *tgt;  // address of the float4 radiance to add to
 };
 
+struct EDL {                // vertices to light, written by shade, read by direct
+  uint32_t *idx;            // index in the shaded queue
+  unsigned long long *tgt;  // address of the float4 radiance their light adds to
+};
+
 __global__ void k_e_plan(EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N, uint32_t cur,
                          uint32_t sp_cap) {
   const uint32_t n_cur = ctl->qcount[cur];
@@ -66,6 +71,7 @@ __global__ void k_e_plan(EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint3
   ctl->qcount[cur] = n_cur + take + uint32_t(n_new);
   ctl->qcount[cur ^ 1u] = 0;
   ctl->scount = 0;
+  ctl->dcount = 0;
   ctl->disp_closest = 0;
   ctl->disp_shadow = 0;
 }
@@ -174,12 +180,11 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_shadow(
 template <bool DIRECT>
 __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
                                                  const DevScene *scenes, EQ qin, const uint32_t *hit_ref,
-                                                 const float *hit_t, EQ qout, ESQ sq,
+                                                 const float *hit_t, EQ qout, EDL dl,
                                                  unsigned long long *job_done, unsigned long long *job_spawned,
                                                  EQ sp, uint32_t sp_cap) {
   const uint32_t n = ctl->qcount[cur];
   uint32_t *count_out = &ctl->qcount[cur ^ 1u];
-  uint32_t *count_sq = &ctl->scount;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -379,6 +384,68 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
       if (fin && lane == uint32_t(__ffs(m) - 1)) atomicAdd(job_done + job, (unsigned long long)__popc(m));
     }
 
+    // Vertices with lights to sample go to the direct-lighting list.
+    const bool lit = alive && J->jc.direct_samples != 0u && s->n_lights != 0u;
+    const uint32_t dslot = warp_append(&ctl->dcount, lit);
+    if (lit) {
+      dl.idx[dslot] = i;
+      dl.tgt[dslot] = reinterpret_cast<unsigned long long>(target);
+    }
+  }
+}
+
+// Direct lighting of the vertices the shading kernel listed, one list entry
+// per thread: the vertex is rebuilt from its queue entry (the same arithmetic
+// as in k_e_shade, so the same bits), then every light is sampled.  Kept out
+// of k_e_shade so neither kernel's body outgrows the instruction cache, and
+// run over a compacted list so escaped and absorbed paths leave no idle lanes.
+template <bool DIRECT>
+__global__ void __launch_bounds__(128, 6) k_e_direct(EngineCtl *ctl, const EngineJobDev *jobs,
+                                                  const DevScene *scenes, EQ qin, const uint32_t *hit_ref,
+                                                  const float *hit_t, EDL dl, ESQ sq) {
+  const uint32_t n = ctl->dcount;
+  uint32_t *count_sq = &ctl->scount;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+
+  for (uint32_t wb = warp * 32; wb < n; wb += nwarps * 32) {
+    const uint32_t k = wb + lane;
+    const bool alive = k < n;
+    uint32_t scene = 0, bounce = 0, pixel = 0, sidx = 0;
+    float3 thr = f3(0, 0, 0);
+    Isec I;
+    BsdfCtx B{nullptr, 1.f, 1.f};
+    DevMedium med{1.f, {0, 0, 0}};
+    const EngineJobDev *J = jobs;
+    const DevScene *s = scenes;
+    Rng rng{0, 0, 0, 0};
+    float4 *target = nullptr;
+    if (alive) {
+      const uint32_t i = dl.idx[k];
+      target = reinterpret_cast<float4 *>(dl.tgt[k]);
+      const uint4 meta = qin.meta[i];
+      const uint32_t ps = meta.x;
+      const unsigned long long g = (unsigned long long)meta.z | ((unsigned long long)meta.w << 32);
+      J = jobs + meta.y;
+      scene = J->scene;
+      s = scenes + scene;
+      const JobConsts &jc = J->jc;
+      const float4 o4 = qin.o[i], d4 = qin.d[i];
+      const float t = hit_t[i];
+      rng = Rng{jc.seed_lo, jc.seed_hi, uint32_t(g), uint32_t(g >> 32)};
+      pixel = uint32_t(g / jc.S);
+      sidx = uint32_t(g % jc.S);
+      bounce = ps_len(ps);
+      const uint32_t depth = ps_depth(ps);
+      med = s->media[depth ? ps_medium(ps, depth - 1) : 0u];
+      thr = mul3(xyz(qin.thr[i]), medium_transmittance(med, length(xyz(d4)) * (t - o4.w)));
+      I = make_isec(*s, hit_ref[i], xyz(o4), xyz(d4), t);
+      B.m = bsdf_material(*s, I.mat);
+      B.medium_ior = med.ior;
+      B.enclosing_ior = depth >= 2 ? s->media[ps_medium(ps, depth - 2)].ior : 1.f;
+    }
+
     // ---- direct lighting (render/direct-illum.cc:83-255) ----------------
     // The light loop bound is the largest in the warp, so shadow-ray appends
     // stay warp-synchronous.
@@ -468,12 +535,12 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
 }
 
 // One iteration's kernel sequence on ST.  EV (null while capturing a graph)
-// receives five events: before plan, before closest, before shade, before
-// shadow, after shadow.
+// receives five events: before plan, before closest, before shade (shading and
+// direct lighting), before shadow, after shadow.
 template <int STACK>
 void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N,
                       uint32_t cur, const EngineJobDev *jobs, const DevScene *scenes, EQ qc, EQ qn,
-                      uint32_t *hit_ref, float *hit_t, ESQ sq, unsigned long long *job_done,
+                      uint32_t *hit_ref, float *hit_t, EDL dl, ESQ sq, unsigned long long *job_done,
                       unsigned long long *job_spawned, EQ sp, uint32_t sp_cap, bool direct,
                       const cudaEvent_t *ev) {
   const uint32_t sms = uint32_t(num_sms());
@@ -484,12 +551,15 @@ void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uin
   k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
                                                                                hit_t);
   if (ev) cudaEventRecord(ev[2], st);
-  if (direct)
-    k_e_shade<true><<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done,
+  if (direct) {
+    k_e_shade<true><<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, dl, job_done,
                                               job_spawned, sp, sp_cap);
-  else
-    k_e_shade<false><<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, sq, job_done,
+    k_e_direct<true><<<sms * 12, 128, 0, st>>>(ctl, jobs, scenes, qc, hit_ref, hit_t, dl, sq);
+  } else {
+    k_e_shade<false><<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, dl, job_done,
                                                job_spawned, sp, sp_cap);
+    k_e_direct<false><<<sms * 12, 128, 0, st>>>(ctl, jobs, scenes, qc, hit_ref, hit_t, dl, sq);
+  }
   if (ev) cudaEventRecord(ev[3], st);
   k_e_shadow<STACK><<<resident_grid(k_e_shadow<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, scenes, sq);
   if (ev) cudaEventRecord(ev[4], st);
@@ -565,7 +635,7 @@ Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
   size_t o_q[2][5];
   for (int k = 0; k < 2; k++)
     for (int a = 0; a < 5; a++) o_q[k][a] = take(16 * N);
-  size_t o_href = take(4 * N), o_ht = take(4 * N);
+  size_t o_href = take(4 * N), o_ht = take(4 * N), o_didx = take(4 * N), o_dtgt = take(8 * N);
   size_t o_so = take(16 * N * 2 * L), o_sd = take(16 * N * 2 * L), o_sc = take(16 * N * 2 * L),
          o_st = take(8 * N * 2 * L);
   // Spawn ring for the direct integrator's second rays: a quarter of the
@@ -592,6 +662,8 @@ Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
   sp_meta_ = reinterpret_cast<uint4 *>(b + o_sp[4]);
   hit_ref_ = reinterpret_cast<uint32_t *>(b + o_href);
   hit_t_ = reinterpret_cast<float *>(b + o_ht);
+  d_idx_ = reinterpret_cast<uint32_t *>(b + o_didx);
+  d_tgt_ = reinterpret_cast<unsigned long long *>(b + o_dtgt);
   s_o_ = reinterpret_cast<float4 *>(b + o_so);
   s_d_ = reinterpret_cast<float4 *>(b + o_sd);
   s_c_ = reinterpret_cast<float4 *>(b + o_sc);
@@ -684,7 +756,7 @@ void Engine::launch_iterations(bool direct) {
     const cudaEvent_t *ev = profile_on_ ? &events_[5 * it] : nullptr;
 #define SNOG_ITER(S)                                                                                          \
   launch_iteration<S>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], \
-                      q[cur ^ 1], hit_ref_, hit_t_, sq, job_done_, job_done_ + cfg_.max_jobs,            \
+                      q[cur ^ 1], hit_ref_, hit_t_, EDL{d_idx_, d_tgt_}, sq, job_done_, job_done_ + cfg_.max_jobs,            \
                       EQ{sp_o_, sp_d_, sp_thr_, sp_rad_, sp_meta_}, sp_cap_, direct, ev)
     switch (graph_stack_) {
       case 32: SNOG_ITER(32); break;
@@ -1005,7 +1077,7 @@ bool Engine::step() {
       if (!graph_[direct]) build_graph(direct);
       check_cuda(cudaGraphLaunch(graph_[direct], stream_), "graph launch");
     }
-    kernel_launches_ += 5 * 2 * cfg_.iters_per_launch;
+    kernel_launches_ += 6 * 2 * cfg_.iters_per_launch;
     check_cuda(cudaMemcpyAsync(ctl_host_, ctl_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_), "ctl");
     check_cuda(cudaMemcpyAsync(done_host_, job_done_, 16 * size_t(cfg_.max_jobs), cudaMemcpyDeviceToHost, stream_),
                "done");

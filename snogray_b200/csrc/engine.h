@@ -72,7 +72,8 @@ struct EngineCtl {
   // queue slot.  Shade appends (spawn_n, up to spawn_room), plan publishes
   // them and hands regen the oldest (regen_spawn from regen_spawn_head).
   unsigned long long spawn_head, spawn_tail, regen_spawn_head;
-  uint32_t spawn_n, spawn_room, regen_spawn, pad_;
+  uint32_t spawn_n, spawn_room, regen_spawn;
+  uint32_t dcount;          // vertices queued for direct lighting this iteration
 };
 
 struct EngineConfigHost {
@@ -223,6 +224,8 @@ class Engine {
   float *hit_t_;
   float4 *s_o_, *s_d_, *s_c_;
   unsigned long long *s_tgt_;
+  uint32_t *d_idx_;                           // direct-lighting list: queue index of the vertex
+  unsigned long long *d_tgt_;                 //   and the radiance its light adds to
   EngineCtl *ctl_;
   WorkItem *ring_;
   EngineJobDev *jobs_dev_;

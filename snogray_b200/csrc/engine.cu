@@ -177,8 +177,14 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_shadow(
 // terrain frame).
 // DIRECT: the direct integrator's code is compiled in (launched while a job
 // of that integrator is active; the path integrator's kernel stays smaller).
+#ifndef SNOG_SHADE_MINBLOCKS
+#define SNOG_SHADE_MINBLOCKS 6
+#endif
+#ifndef SNOG_DIRECT_MINBLOCKS
+#define SNOG_DIRECT_MINBLOCKS 6
+#endif
 template <bool DIRECT>
-__global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
+__global__ void __launch_bounds__(128, SNOG_SHADE_MINBLOCKS) k_e_shade(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
                                                  const DevScene *scenes, EQ qin, const uint32_t *hit_ref,
                                                  const float *hit_t, EQ qout, EDL dl,
                                                  unsigned long long *job_done, unsigned long long *job_spawned,
@@ -400,7 +406,7 @@ __global__ void __launch_bounds__(128, 6) k_e_shade(EngineCtl *ctl, uint32_t cur
 // of k_e_shade so neither kernel's body outgrows the instruction cache, and
 // run over a compacted list so escaped and absorbed paths leave no idle lanes.
 template <bool DIRECT>
-__global__ void __launch_bounds__(128, 6) k_e_direct(EngineCtl *ctl, const EngineJobDev *jobs,
+__global__ void __launch_bounds__(128, SNOG_DIRECT_MINBLOCKS) k_e_direct(EngineCtl *ctl, const EngineJobDev *jobs,
                                                   const DevScene *scenes, EQ qin, const uint32_t *hit_ref,
                                                   const float *hit_t, EDL dl, ESQ sq) {
   const uint32_t n = ctl->dcount;

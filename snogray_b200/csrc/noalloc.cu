@@ -92,6 +92,8 @@ void carve_waves(WaveBuffers &wb, char *base, size_t bytes, uint64_t cap, uint32
   wb.hit_ref = reinterpret_cast<uint32_t *>(take(4 * cap));
   wb.hit_t = reinterpret_cast<float *>(take(4 * cap));
   wb.jit = reinterpret_cast<float2 *>(take(8 * cap));
+  wb.d_idx = reinterpret_cast<uint32_t *>(take(4 * cap));
+  wb.d_thr = reinterpret_cast<float4 *>(take(16 * cap));
   wb.s_o = reinterpret_cast<float4 *>(take(16 * cap * 2 * nl));
   wb.s_d = reinterpret_cast<float4 *>(take(16 * cap * 2 * nl));
   wb.s_c = reinterpret_cast<float4 *>(take(16 * cap * 2 * nl));

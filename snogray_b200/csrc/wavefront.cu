@@ -7,10 +7,12 @@
 //   k_camera                 eye rays for every path (camera/camera.cc:108-160)
 //   per bounce b = 0..max_len:
 //     k_trace_closest        octree closest hit for the live rays
-//     k_shade                emission, direct lighting with MIS (emits
-//                            shadow rays), BSDF continuation, Russian
+//     k_shade                emission, BSDF continuation, Russian
 //                            roulette; appends surviving rays to the other
-//                            queue with warp-aggregated atomics
+//                            queue with warp-aggregated atomics and lists
+//                            the vertices to light
+//     k_direct               direct lighting with MIS of the listed
+//                            vertices (emits shadow rays)
 //     k_trace_shadow         any-hit for the shadow rays; unoccluded ones add
 //                            their contribution to the path's radiance
 //   k_splat                  Mitchell filter gather of the wave's samples
@@ -48,6 +50,10 @@ struct RayQ {
 };
 struct ShadowQ {
   float4 *o, *d, *c;
+};
+struct DirectL {             // vertices to light, written by k_shade
+  uint32_t *idx;             // queue index
+  float4 *thr;               // throughput before the continuation, path state word in w
 };
 
 // ---- kernels -----------------------------------------------------------------
@@ -111,6 +117,7 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_clo
     counters[cur ^ 1u] = 0;   // next queue and shadow queue start empty
     counters[2] = 0;
     counters[5] = 0;          // shadow kernel's dispenser
+    counters[6] = 0;          // direct-lighting list
     stats[0] += n;
   }
   TraceCounters c{0, 0, 0};
@@ -156,23 +163,19 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_sha
   if (prof) warp_count(stats + 4, c.nodes, c.tests);
 }
 
-// 6 blocks of 128 per SM (80 registers), as the engine's shading kernel.
+// 6 blocks of 128 per SM (80 registers), as the engine's shading kernels.
 __global__ void __launch_bounds__(128, 6) k_shade(DevScene s, JobConsts jc, uint64_t base, uint32_t bounce,
                                                RayQ qin, uint32_t *counters, uint32_t cur,
                                                const uint32_t *hit_ref, const float *hit_t, PathPtrs P,
-                                               RayQ qout, ShadowQ sq) {
+                                               RayQ qout, DirectL dl) {
   const uint32_t n = counters[cur];
   if (blockIdx.x == 0 && threadIdx.x == 0) counters[4] = 0;   // next bounce's dispenser
   uint32_t *count_out = counters + (cur ^ 1u);
-  uint32_t *count_sq = counters + 2;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const Strata st = strata_for(jc.S);
-  const Strata st_direct = strata_for(jc.S * (jc.direct_samples ? jc.direct_samples : 1));
-  const Strata st_rand = strata_for(jc.direct_samples ? jc.direct_samples : 1);
   const bool strat = bounce < jc.min_len;
-  const float inv_ns = jc.direct_samples ? 1.f / float(jc.direct_samples) : 0.f;
 
   for (uint32_t wb = warp * 32; wb < n; wb += nwarps * 32) {
     const uint32_t i = wb + lane;
@@ -229,6 +232,111 @@ __global__ void __launch_bounds__(128, 6) k_shade(DevScene s, JobConsts jc, uint
           alive = true;
         }
       }
+    }
+
+    // Vertices with lights to sample go to the direct-lighting list, with the
+    // throughput and path state the continuation below replaces.
+    const bool lit = alive && jc.direct_samples != 0u && s.n_lights != 0u;
+    const uint32_t dslot = warp_append(counters + 6, lit);
+    if (lit) {
+      dl.idx[dslot] = i;
+      dl.thr[dslot] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(ps));
+    }
+
+    // ---- BSDF continuation, roulette, next ray (path-integ.cc:309-403) ----
+    bool cont = false;
+    float3 next_d = f3(0, 0, 0);
+    if (alive) {
+      const uint32_t len = ps_len(ps);
+      float2 prm = strat ? strat_uv(st, rng, pixel, sidx, dim_of(bounce, K_BSDF)) : rng.uv(dim_of(bounce, K_BSDF));
+      BSample bs = bsdf_sample(B, I, prm, B_ALL);
+      if (bs.pdf != 0.f && !(bs.val.x == 0.f && bs.val.y == 0.f && bs.val.z == 0.f)) {
+        thr = mul3(thr, mul(bs.val, fabsf(I.cos_n(bs.dir)) / bs.pdf));
+        bool stop = false;
+        if (len > jc.min_len) {
+          float p = fminf(intensity(thr) * rr_ratio, 1.f);
+          if (rng.u(dim_of(bounce, K_RR)) > p) {
+            stop = true;
+          } else {
+            thr = mul(thr, 1.f / p);
+            rr_ratio *= p;
+          }
+        }
+        if (!stop && len != jc.max_len) {
+          cont = true;
+          next_d = I.nf.from(bs.dir);
+          uint32_t nps = (ps & ~0x1ffu) | (len + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
+          if (bs.flags & B_TRANSMISSIVE) {
+            uint32_t mid = s.mats[I.mat].medium_id;
+            if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
+          }
+          ps = nps;
+        }
+      }
+    }
+    uint32_t slot = warp_append(count_out, cont);
+    if (cont) {
+      // Intersect::recursive_ray (dir) (render/intersect.cc:196-202)
+      qout.o[slot] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
+      qout.d[slot] = make_float4(next_d.x, next_d.y, next_d.z, jc.horizon);
+      qout.path[slot] = path;
+    }
+    if (active) {
+      P.rad[path] = make_float4(rad.x, rad.y, rad.z, alpha);
+      if (cont) {
+        P.thr[path] = make_float4(thr.x, thr.y, thr.z, rr_ratio);
+        P.pstate[path] = ps;
+      }
+    }
+  }
+}
+
+// Direct lighting of the vertices k_shade listed (render/direct-illum.cc:83-255),
+// one list entry per thread: the vertex is rebuilt from its queue entry (the
+// same arithmetic as in k_shade, so the same bits) and every light sampled.
+// Kept out of k_shade so neither body outgrows the instruction cache, and run
+// over a compacted list so escaped and absorbed paths leave no idle lanes.
+__global__ void __launch_bounds__(128, 6) k_direct(DevScene s, JobConsts jc, uint64_t base, uint32_t bounce,
+                                                RayQ qin, uint32_t *counters, const uint32_t *hit_ref,
+                                                const float *hit_t, DirectL dl, ShadowQ sq) {
+  const uint32_t n = counters[6];
+  uint32_t *count_sq = counters + 2;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const Strata st_direct = strata_for(jc.S * (jc.direct_samples ? jc.direct_samples : 1));
+  const Strata st_rand = strata_for(jc.direct_samples ? jc.direct_samples : 1);
+  const bool strat = bounce < jc.min_len;
+  const float inv_ns = jc.direct_samples ? 1.f / float(jc.direct_samples) : 0.f;
+
+  for (uint32_t wb = warp * 32; wb < n; wb += nwarps * 32) {
+    const uint32_t k = wb + lane;
+    const bool alive = k < n;
+    uint32_t path = 0;
+    float3 thr = f3(0, 0, 0);
+    Isec I;
+    BsdfCtx B{nullptr, 1.f, 1.f};
+    DevMedium med{1.f, {0, 0, 0}};
+    Rng rng{jc.seed_lo, jc.seed_hi, 0, 0};
+    uint32_t pixel = 0, sidx = 0;
+    if (alive) {
+      const uint32_t i = dl.idx[k];
+      const float4 t4 = dl.thr[k];
+      thr = xyz(t4);
+      const uint32_t ps = __float_as_uint(t4.w);
+      path = qin.path[i];
+      const float4 o4 = qin.o[i], d4 = qin.d[i];
+      const uint64_t g = base + path;
+      pixel = uint32_t(g / jc.S);
+      sidx = uint32_t(g % jc.S);
+      rng.path_lo = uint32_t(g);
+      rng.path_hi = uint32_t(g >> 32);
+      const uint32_t depth = ps_depth(ps);
+      med = s.media[depth ? ps_medium(ps, depth - 1) : 0u];
+      I = make_isec(s, hit_ref[i], xyz(o4), xyz(d4), hit_t[i]);
+      B.m = bsdf_material(s, I.mat);
+      B.medium_ior = med.ior;
+      B.enclosing_ior = depth >= 2 ? s.media[ps_medium(ps, depth - 2)].ior : 1.f;
     }
 
     // ---- direct lighting (render/direct-illum.cc:83-255) ----------------
@@ -311,51 +419,6 @@ __global__ void __launch_bounds__(128, 6) k_shade(DevScene s, JobConsts jc, uint
       }
     }
 
-    // ---- BSDF continuation, roulette, next ray (path-integ.cc:309-403) ----
-    bool cont = false;
-    float3 next_d = f3(0, 0, 0);
-    if (alive) {
-      const uint32_t len = ps_len(ps);
-      float2 prm = strat ? strat_uv(st, rng, pixel, sidx, dim_of(bounce, K_BSDF)) : rng.uv(dim_of(bounce, K_BSDF));
-      BSample bs = bsdf_sample(B, I, prm, B_ALL);
-      if (bs.pdf != 0.f && !(bs.val.x == 0.f && bs.val.y == 0.f && bs.val.z == 0.f)) {
-        thr = mul3(thr, mul(bs.val, fabsf(I.cos_n(bs.dir)) / bs.pdf));
-        bool stop = false;
-        if (len > jc.min_len) {
-          float p = fminf(intensity(thr) * rr_ratio, 1.f);
-          if (rng.u(dim_of(bounce, K_RR)) > p) {
-            stop = true;
-          } else {
-            thr = mul(thr, 1.f / p);
-            rr_ratio *= p;
-          }
-        }
-        if (!stop && len != jc.max_len) {
-          cont = true;
-          next_d = I.nf.from(bs.dir);
-          uint32_t nps = (ps & ~0x1ffu) | (len + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
-          if (bs.flags & B_TRANSMISSIVE) {
-            uint32_t mid = s.mats[I.mat].medium_id;
-            if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
-          }
-          ps = nps;
-        }
-      }
-    }
-    uint32_t slot = warp_append(count_out, cont);
-    if (cont) {
-      // Intersect::recursive_ray (dir) (render/intersect.cc:196-202)
-      qout.o[slot] = make_float4(I.pos.x, I.pos.y, I.pos.z, jc.min_trace);
-      qout.d[slot] = make_float4(next_d.x, next_d.y, next_d.z, jc.horizon);
-      qout.path[slot] = path;
-    }
-    if (active) {
-      P.rad[path] = make_float4(rad.x, rad.y, rad.z, alpha);
-      if (cont) {
-        P.thr[path] = make_float4(thr.x, thr.y, thr.z, rr_ratio);
-        P.pstate[path] = ps;
-      }
-    }
   }
 }
 
@@ -450,12 +513,14 @@ void launch_bounce(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, uint
   RayQ qin{wb.q_o[cur], wb.q_d[cur], wb.q_path[cur]};
   RayQ qout{wb.q_o[cur ^ 1], wb.q_d[cur ^ 1], wb.q_path[cur ^ 1]};
   ShadowQ sq{wb.s_o, wb.s_d, wb.s_c};
+  DirectL dl{wb.d_idx, wb.d_thr};
   PathPtrs P{wb.thr, wb.rad, wb.pstate, wb.jit};
   const bool pf = prof != nullptr;
   if (pf) prof->begin(st, RenderProfile::CLOSEST);
   k_trace_closest<STACK><<<resident_grid(k_trace_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
   if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADE);
-  k_shade<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, P, qout, sq);
+  k_shade<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, P, qout, dl);
+  k_direct<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, wb.hit_ref, wb.hit_t, dl, sq);
   if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADOW);
   k_trace_shadow<STACK><<<resident_grid(k_trace_shadow<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(s, sq, wb.counters, wb.rad, wb.stats, pf);
   if (pf) prof->end(st);
@@ -511,8 +576,8 @@ RenderProfile::~RenderProfile() {
 
 uint64_t wave_bytes_per_path(uint32_t n_lights) {
   // thr 16 + rad 16 + pstate 4 + 2 queues x 36 + hit 8 + jitter 8
-  // + shadow queue 48 per entry, 2 entries per light sample
-  return 16 + 16 + 4 + 72 + 8 + 8 + 48ull * 2 * (n_lights ? n_lights : 1);
+  // + direct-lighting list 20 + shadow queue 48 per entry, 2 entries per light sample
+  return 16 + 16 + 4 + 72 + 8 + 8 + 20 + 48ull * 2 * (n_lights ? n_lights : 1);
 }
 
 cudaError_t wave_alloc(WaveBuffers &wb, uint64_t cap, uint32_t n_lights) {
@@ -528,6 +593,7 @@ cudaError_t wave_alloc(WaveBuffers &wb, uint64_t cap, uint32_t n_lights) {
   size_t o_qo0 = take(16 * cap), o_qd0 = take(16 * cap), o_qp0 = take(4 * cap);
   size_t o_qo1 = take(16 * cap), o_qd1 = take(16 * cap), o_qp1 = take(4 * cap);
   size_t o_href = take(4 * cap), o_ht = take(4 * cap), o_jit = take(8 * cap);
+  size_t o_didx = take(4 * cap), o_dthr = take(16 * cap);
   size_t o_so = take(16 * cap * 2 * nl), o_sd = take(16 * cap * 2 * nl), o_sc = take(16 * cap * 2 * nl);
   size_t o_cnt = take(64), o_stats = take(64);
   char *base = nullptr;
@@ -549,6 +615,8 @@ cudaError_t wave_alloc(WaveBuffers &wb, uint64_t cap, uint32_t n_lights) {
   wb.hit_ref = reinterpret_cast<uint32_t *>(base + o_href);
   wb.hit_t = reinterpret_cast<float *>(base + o_ht);
   wb.jit = reinterpret_cast<float2 *>(base + o_jit);
+  wb.d_idx = reinterpret_cast<uint32_t *>(base + o_didx);
+  wb.d_thr = reinterpret_cast<float4 *>(base + o_dthr);
   wb.s_o = reinterpret_cast<float4 *>(base + o_so);
   wb.s_d = reinterpret_cast<float4 *>(base + o_sd);
   wb.s_c = reinterpret_cast<float4 *>(base + o_sc);
@@ -631,7 +699,7 @@ cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, 
         case 256: launch_bounce<256>(s, jc, wb, base, b, cur, grid128, st, prof); break;
         default: return cudaErrorInvalidValue;
       }
-      nl += 3;
+      nl += 4;
     }
     // Output rows reached by this wave's pattern rows.
     const uint32_t p0 = uint32_t(base / jc.S), p1 = uint32_t((base + n) / jc.S);

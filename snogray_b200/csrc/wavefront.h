@@ -38,8 +38,11 @@ struct WaveBuffers {
   uint32_t *hit_ref = nullptr;               // per queue slot
   float *hit_t = nullptr;
   float2 *jit = nullptr;                     // per path: camera jitter (splat reuses it)
+  uint32_t *d_idx = nullptr;                 // direct-lighting list: queue index,
+  float4 *d_thr = nullptr;                   //   throughput and path state of each lit vertex
   float4 *s_o = nullptr, *s_d = nullptr, *s_c = nullptr;   // shadow queue (c.w = path id)
-  uint32_t *counters = nullptr;              // [0,1] ray queues, [2] shadow queue, [3] error flags
+  uint32_t *counters = nullptr;              // [0,1] ray queues, [2] shadow queue, [3] error flags,
+                                             // [4,5] trace dispensers, [6] direct-lighting list
   unsigned long long *stats = nullptr;       // [0] closest rays, [1] shadow rays
   uint64_t bytes = 0;
   void *block = nullptr;

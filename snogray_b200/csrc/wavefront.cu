@@ -438,13 +438,23 @@ __device__ __forceinline__ float mitchell1(float x) {
 // (ImageFilterConv::add_sample, image/image-filter-conv.h:109-186): every
 // sample within the filter's support of a target pixel centre adds
 // Tint * w and w, with the negative-lobe clamp (neg_clamp = -0.1).
+// G lanes (a power of two up to 32) per target pixel: they take every G-th
+// sample of each neighbouring pattern pixel -- consecutive samples, so the
+// group's loads coalesce -- and sum their shares with shuffles.  With one
+// thread per pixel a small image at high spp left most of the GPU idle on
+// long chains of loads.
+template <int G>
 __global__ void __launch_bounds__(256) k_splat(JobConsts jc, uint64_t base, uint32_t n, const float4 *rad,
                                                const float2 *jit, float4 *accum, float *wsum, int ty0,
                                                int nrows) {
   const uint32_t p0 = uint32_t(base / jc.S), p1 = uint32_t((base + n) / jc.S);
   const uint32_t total = uint32_t(nrows) * jc.W;
   const float neg_clamp = -0.1f;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+  const uint32_t sub = threadIdx.x & uint32_t(G - 1);
+  const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~uint32_t(G - 1)));
+  const uint32_t groups = (gridDim.x * blockDim.x) / G;
+  // Every lane of a group has the same T, so a group runs its loop together.
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G; t < total; t += groups) {
     const int tx = int(t % jc.W), ty = ty0 + int(t / jc.W);
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     float wacc = 0.f;
@@ -457,7 +467,7 @@ __global__ void __launch_bounds__(256) k_splat(JobConsts jc, uint64_t base, uint
         const uint32_t pidx = uint32_t(row) * jc.PW + uint32_t(col);
         if (pidx < p0 || pidx >= p1) continue;
         const uint32_t pbase = (pidx - p0) * jc.S;
-        for (uint32_t k = 0; k < jc.S; k++) {
+        for (uint32_t k = sub; k < jc.S; k += G) {
           float2 j = jit[pbase + k];
           float sx = float(tx + dx) + j.x, sy = float(ty + dy) + j.y;
           float w = mitchell1(sx - (float(tx) + 0.5f)) * mitchell1(sy - (float(ty) + 0.5f));
@@ -478,11 +488,32 @@ __global__ void __launch_bounds__(256) k_splat(JobConsts jc, uint64_t base, uint
         }
       }
     }
-    const size_t o = size_t(ty) * jc.W + size_t(tx);
-    float4 a = accum[o];
-    accum[o] = make_float4(a.x + acc.x, a.y + acc.y, a.z + acc.z, a.w + acc.w);
-    wsum[o] += wacc;
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) {
+      acc.x += __shfl_xor_sync(gmask, acc.x, off);
+      acc.y += __shfl_xor_sync(gmask, acc.y, off);
+      acc.z += __shfl_xor_sync(gmask, acc.z, off);
+      acc.w += __shfl_xor_sync(gmask, acc.w, off);
+      wacc += __shfl_xor_sync(gmask, wacc, off);
+    }
+    if (sub == 0) {
+      const size_t o = size_t(ty) * jc.W + size_t(tx);
+      float4 a = accum[o];
+      accum[o] = make_float4(a.x + acc.x, a.y + acc.y, a.z + acc.z, a.w + acc.w);
+      wsum[o] += wacc;
+    }
   }
+}
+
+// The splat with the lane group that fits S samples per pixel.
+void launch_splat(const JobConsts &jc, uint64_t base, uint32_t n, const float4 *rad, const float2 *jit,
+                  float4 *accum, float *wsum, int ty0, int nrows, uint32_t grid256, cudaStream_t st) {
+  if (jc.S >= 32) k_splat<32><<<grid256, 256, 0, st>>>(jc, base, n, rad, jit, accum, wsum, ty0, nrows);
+  else if (jc.S > 8) k_splat<16><<<grid256, 256, 0, st>>>(jc, base, n, rad, jit, accum, wsum, ty0, nrows);
+  else if (jc.S > 4) k_splat<8><<<grid256, 256, 0, st>>>(jc, base, n, rad, jit, accum, wsum, ty0, nrows);
+  else if (jc.S > 2) k_splat<4><<<grid256, 256, 0, st>>>(jc, base, n, rad, jit, accum, wsum, ty0, nrows);
+  else if (jc.S > 1) k_splat<2><<<grid256, 256, 0, st>>>(jc, base, n, rad, jit, accum, wsum, ty0, nrows);
+  else k_splat<1><<<grid256, 256, 0, st>>>(jc, base, n, rad, jit, accum, wsum, ty0, nrows);
 }
 
 // ImageSampledOutput::set_raw_min_y row flush (image/image-sampled-output.cc:79-123).
@@ -707,7 +738,7 @@ cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, 
     int ty0 = r0 - 4 < 0 ? 0 : r0 - 4, ty1 = r1 > int(jc.H) - 1 ? int(jc.H) - 1 : r1;
     if (ty1 >= ty0) {
       if (prof) prof->begin(st, RenderProfile::OTHER);
-      k_splat<<<grid256, 256, 0, st>>>(jc, base, n, wb.rad, P.jit, accum, wsum, ty0, ty1 - ty0 + 1);
+      launch_splat(jc, base, n, wb.rad, P.jit, accum, wsum, ty0, ty1 - ty0 + 1, grid256, st);
       if (prof) prof->end(st);
       nl++;
     }
@@ -732,7 +763,7 @@ cudaError_t splat_job(const JobConsts &jc, const float4 *rad, const float2 *jit,
   if (e == cudaSuccess) e = cudaMemsetAsync(wsum, 0, npix * sizeof(float), st);
   if (e != cudaSuccess) return e;
   const uint32_t grid256 = uint32_t(num_sms()) * 8;
-  k_splat<<<grid256, 256, 0, st>>>(jc, 0, uint32_t(total), rad, jit, accum, wsum, 0, int(jc.H));
+  launch_splat(jc, 0, uint32_t(total), rad, jit, accum, wsum, 0, int(jc.H), grid256, st);
   k_resolve<<<grid256, 256, 0, st>>>(uint32_t(npix), accum, wsum, out_rgb);
   return cudaGetLastError();
 }

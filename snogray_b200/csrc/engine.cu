@@ -171,10 +171,11 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_shadow(
   if (c.overflow) atomicOr(&ctl->err, 1u);
 }
 
-// 6 blocks of 128 per SM (80 registers): the kernel's long, divergent body
-// stalls on instruction fetch, and more resident warps hide that better than
-// the spill-free 117-register build at 4 blocks (measured 104 -> 88 ms per
-// terrain frame).
+// Shading, first half: emission, the continuation sample and roulette; the
+// vertices to light go to a list for k_e_direct.  6 blocks of 128 per SM (80
+// registers) for both halves: the bodies are long and divergent, and more
+// resident warps hide their instruction-fetch stalls (4 or 5 blocks for
+// k_e_direct, 8 for k_e_shade measured 0.6-2 % slower on the terrain frame).
 // DIRECT: the direct integrator's code is compiled in (launched while a job
 // of that integrator is active; the path integrator's kernel stays smaller).
 #ifndef SNOG_SHADE_MINBLOCKS

@@ -53,14 +53,37 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 WIDTH, HEIGHT, SPP, MAX_LEN = 1920, 1080, 64, 16
+REF_SPP = 2          # samples per pixel of each reference step (a bounded sample of the job)
 METRIC = "Mpaths/s at matched RMSE (terrain 1920x1080, 64 spp, depth 16)"
 
 
+def scenes_module():
+    """snogray_b200/scenes.py (numpy only), loaded from its file: the
+    reference arm must not import the package, whose __init__ maps the CUDA
+    library into the process."""
+    import importlib.util
+    if "snogray_b200.scenes" in sys.modules:
+        return sys.modules["snogray_b200.scenes"]
+    if "_snog_scenes_file" not in sys.modules:
+        spec_ = importlib.util.spec_from_file_location("_snog_scenes_file",
+                                                       os.path.join(HERE, "snogray_b200", "scenes.py"))
+        mod = importlib.util.module_from_spec(spec_)
+        sys.modules["_snog_scenes_file"] = mod
+        spec_.loader.exec_module(mod)
+    return sys.modules["_snog_scenes_file"]
+
+
 def workload():
-    from snogray_b200 import scenes
+    scenes = scenes_module()
     sd = scenes.terrain_scene()
     cam = scenes.terrain_camera(WIDTH, HEIGHT)
     return sd, cam
+
+
+def workload_config():
+    """The `config` both arms print (the workload, nothing arm-specific)."""
+    return {"workload": "terrain-2M-tris+200-spheres+sky-envmap", "width": WIDTH, "height": HEIGHT,
+            "spp": SPP, "max_path_len": MAX_LEN}
 
 
 def max_over_ranks(x, dist=None):
@@ -188,25 +211,28 @@ def bench_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "compiled reference (oracle/_ref/snog_ref_base) not present"}))
         return 0
-    from snogray_b200 import scenes
+    scenes = scenes_module()
     sd, cam = workload()
     params = scenes.terrain_params(WIDTH, HEIGHT, SPP)
     threads = os.cpu_count() or 1
-    spp_sample = 1
-    recs = run_reference(sd, cam, params, spp_sample, args.warmup + args.steps, threads)
+    # Each step renders the whole image at REF_SPP samples per pixel: a
+    # bounded sample of the 64-spp job (the rate per path does not depend on
+    # the spp, which only repeats the same per-pixel work).
+    recs = run_reference(sd, cam, params, REF_SPP, args.warmup + args.steps, threads)
     timed = recs[args.warmup:]
     secs = sum(r["seconds"] for r in timed)
     paths = sum(r["paths"] for r in timed)
     value = paths / secs * 1e-6
     ms_per_step = secs / len(timed) * 1e3
-    sample = f"{WIDTH}x{HEIGHT} at {spp_sample} spp per step (of {SPP}), all rows"
+    sample = (f"{WIDTH}x{HEIGHT} (all rows) at {REF_SPP} spp per step of the {SPP}-spp job, "
+              f"reference compiled with its own flags, {threads} threads")
     line = {"metric": METRIC, "value": round(value, 4), "unit": "Mpaths/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "terrain-2M-tris+200-spheres+sky-envmap", "width": WIDTH,
-                       "height": HEIGHT, "spp": SPP, "max_path_len": MAX_LEN,
-                       "sample_spp_per_step": spp_sample},
+            "config": workload_config(),
+            "sample": {"spp_per_step": REF_SPP, "paths_per_step": int(paths / len(timed)),
+                       "threads": threads},
             "cpu_baseline": {"value": round(value, 4), "unit": "Mpaths/s", "cores": threads,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": round(value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
@@ -244,15 +270,93 @@ def bench_isec(args, n_tri=1 << 20, n_rays=1 << 24):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
-    sample = rays[:, :65536].cpu().numpy()
-    _, _, _, cnt = sc.trace(sample, 32768)
+    half = 65536
+    sample = torch.cat([rays[:, :half], rays[:, nc:nc + half]], 1).cpu().numpy()
+    _, _, _, cnt = sc.trace(sample, half)
     out = {"workload": f"{n_tri} random triangles, {n_rays} rays (half closest, half any)",
            "mrays_per_s": round(n_rays / ms * 1e-3, 2), "ms_per_launch": round(ms, 3),
            "hit_rate_closest": round(float((prim[:nc] >= 0).float().mean()), 4),
-           "nodes_per_ray": round((cnt["closest_nodes"] + cnt["any_nodes"]) / 65536, 2),
-           "tests_per_ray": round((cnt["closest_tests"] + cnt["any_tests"]) / 65536, 2)}
+           "nodes_per_ray": round((cnt["closest_nodes"] + cnt["any_nodes"]) / (2 * half), 2),
+           "tests_per_ray": round((cnt["closest_tests"] + cnt["any_tests"]) / (2 * half), 2)}
     sc.close()
+    # Roofline on the reference's own traversal counts for the same rays
+    # (a sample of each half): bytes per query as for the path tracer.
+    ok, spec = ref_available()
+    if ok:
+        _, _, _, st, _ = spec.ref_trace(sd, sample, half, threads=os.cpu_count() or 8, flavour="base")
+        b = []
+        for kind in ("closest", "any"):
+            c = st[kind]
+            b.append(36 + (36 * c["node_calls"] + 4 * (c["surface_tests"] + c["neg_cache_hits"])
+                           + 36 * c["surface_tests"]) / half)
+        alg = b[0] * nc + b[1] * (n_rays - nc)
+        achieved = alg / (ms * 1e-3) / 1e9
+        peak, src = hbm_peak()
+        out["roofline"] = {"bound": "hbm", "kernel": "k_trace_batch", "achieved": round(achieved, 1),
+                           "peak": peak, "peak_source": src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                           "bytes_per_ray": {"closest": round(b[0], 1), "any": round(b[1], 1)},
+                           "bytes_source": "reference traversal counts (RenderStats::IsecStats) on "
+                                           f"{2 * half} of the rays"}
     return out
+
+
+def hbm_peak():
+    """The measured copy bandwidth (MEASURED_PEAKS.json), else the fallback."""
+    pk_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        with open(pk_path) as f:
+            peaks = json.load(f)
+        if "hbm_gbs" in peaks:
+            return float(peaks["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def bench_cornell(args, sb, scenes, torch, stream, reps=5):
+    """The Cornell workload at its stated size (256x256, 16 spp, max depth 8):
+    one job on the plain renderer and on the streaming engine, device time
+    per job, and the reference on the host's cores."""
+    w = h = 256
+    spp = 16
+    sd = scenes.cornell_box()
+    cam = scenes.cornell_camera(w, h)
+    params = scenes.cornell_params(w, h, spp, seed=1)
+    sc = sb.Scene(sd)
+    out = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+    sptr = stream.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        sc.render_device(cam, params, out.data_ptr(), sptr)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        sc.render_device(cam, params, out.data_ptr(), sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / reps
+    job = [(sc, cam, params)]
+    with sb.Engine(sb.engine_config(max_lights=1, slots=1 << 20), stream=sptr) as eng:
+        for _ in range(3):
+            eng.render(job, device_outs=[out.data_ptr()])
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            eng.render(job, device_outs=[out.data_ptr()])
+        e1.record(stream)
+        torch.cuda.synchronize()
+    eng_ms = e0.elapsed_time(e1) / reps
+    sc.close()
+    paths = w * h * spp
+    res = {"workload": "Cornell box (10 tris, Lambert + Glass spheres, 0.25x0.25 area light), 256x256, "
+                       "16 spp, depth 8", "paths": paths,
+           "plain_mpaths_per_s": round(paths / plain_ms * 1e-3, 2), "plain_ms": round(plain_ms, 3),
+           "engine_mpaths_per_s": round(paths / eng_ms * 1e-3, 2), "engine_ms": round(eng_ms, 3)}
+    ok, _ = ref_available()
+    if ok and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = run_reference(sd, cam, params, spp, 2, threads)[-1]
+        res["reference_cpu"] = {"mpaths_per_s": round(r["mpaths_per_s"], 3), "cores": threads,
+                                "seconds": round(r["seconds"], 3)}
+    return res
 
 
 def _cfg_dict(cfg):
@@ -380,12 +484,27 @@ def bench_serve(args, sb, scenes):
             with lock:
                 lat_p.append((time.perf_counter() - t_start - r.arrival_s) * 1e3)
         span_p = time.perf_counter() - t_start
+        # per scene-size class: where the served path gains or loses
+        by_class = {}
+        for k, n_tri in enumerate(scenes.SERVE_SIZES):
+            idx = [i for i, r in enumerate(reqs) if r.scene == k]
+            if not idx:
+                continue
+            by_class[str(n_tri)] = {
+                "requests": len(idx),
+                "paths": int(sum(reqs[i].params.width * reqs[i].params.height * reqs[i].params.spp
+                                 for i in idx)),
+                "served_p50_ms": _pct([lat_s[i] for i in idx], 50),
+                "served_p99_ms": _pct([lat_s[i] for i in idx], 99),
+                "plain_p50_ms": _pct([lat_p[i] for i in idx], 50),
+                "plain_p99_ms": _pct([lat_p[i] for i in idx], 99)}
         out["rates"].append({
             "rate_req_per_s": rate, "paths": paths,
             "served": {"p50_ms": _pct(lat_s, 50), "p95_ms": _pct(lat_s, 95), "p99_ms": _pct(lat_s, 99),
                        "mpaths_per_s": round(paths / span_s * 1e-6, 2), "makespan_s": round(span_s, 2)},
             "plain": {"p50_ms": _pct(lat_p, 50), "p95_ms": _pct(lat_p, 95), "p99_ms": _pct(lat_p, 99),
-                      "mpaths_per_s": round(paths / span_p * 1e-6, 2), "makespan_s": round(span_p, 2)}})
+                      "mpaths_per_s": round(paths / span_p * 1e-6, 2), "makespan_s": round(span_p, 2)},
+            "by_scene_triangles": by_class})
     for h in handles:
         h.close()
     return out
@@ -503,13 +622,7 @@ def bench_ours(args):
                        "kind": "reference",
                        "sample": f"{WIDTH}x{HEIGHT} at 2 spp (of {SPP}), all rows, "
                                  f"{r['seconds']:.1f} s"}
-    peaks = {}
-    pk_path = os.path.join(HERE, "MEASURED_PEAKS.json")
-    if os.path.exists(pk_path):
-        with open(pk_path) as f:
-            peaks = json.load(f)
-    peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    peak, peak_src = hbm_peak()
     roofline = None
     if prof["iterations"] and prof["closest_ms"] > 0:
         per_launch_ms = prof["closest_ms"] / prof["iterations"]
@@ -531,11 +644,22 @@ def bench_ours(args):
                              "bytes_per_ray": round(b_ray, 1)})
         else:
             roofline.update({"achieved": None, "frac": None})
+        if bytes_ray is not None and prof["shadow_ms"] > 0:
+            # the any-hit kernel on the same step, by the same accounting
+            sh_ms = prof["shadow_ms"] / prof["iterations"]
+            sh_rays = prof["shadow_rays"] / prof["iterations"]
+            sh_ach = bytes_ray[1] * sh_rays / (sh_ms * 1e-3) / 1e9
+            roofline["shadow"] = {"kernel": "k_e_shadow", "achieved": round(sh_ach, 1),
+                                  "frac": round(sh_ach / peak, 4), "bytes_per_ray": round(bytes_ray[1], 1),
+                                  "rays_per_launch": round(sh_rays), "ms_per_launch": round(sh_ms, 4)}
         roofline["traffic"] = round(traffic_ray * rays_per_launch) if traffic_ray else None
         roofline["traffic_per_ray"] = traffic_ray
 
-    batched = serve = None
+    batched = serve = isec = cornell = None
     if rank == 0 and ws == 1:
+        if not args.no_extra:
+            cornell = bench_cornell(args, sb, scenes, torch, stream)
+            isec = bench_isec(args)
         if args.batch_jobs:
             batched = bench_batch(args, sb, scenes, torch, stream)
         if args.serve_requests:
@@ -546,10 +670,9 @@ def bench_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded terrain scene; inputs larger than L2, no flush)",
-                "config": {"workload": "terrain-2M-tris+200-spheres+sky-envmap", "width": WIDTH,
-                           "height": HEIGHT, "spp": SPP, "max_path_len": MAX_LEN,
-                           "parallelism": f"replicas x{ws}", "l2": "working set > L2",
-                           "engine": _cfg_dict(cfg)},
+                "config": workload_config(),
+                "parallelism": f"replicas x{ws}", "l2": "working set > L2 (no flush needed)",
+                "engine": _cfg_dict(cfg),
                 "gpu_launches": launches,
                 "e2e": {"value": round(e2e_value, 4), "unit": "Mpaths/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
@@ -559,7 +682,7 @@ def bench_ours(args):
                 "rays": {"closest_per_step": rays[0] // max(args.steps, 1),
                          "shadow_per_step": rays[1] // max(args.steps, 1),
                          "mrays_per_s": round((rays[0] + rays[1]) * ws / (ms * args.steps) * 1e-3, 2)},
-                "batched": batched, "serve": serve}
+                "cornell": cornell, "isec": isec, "batched": batched, "serve": serve}
         print(json.dumps(line))
     scene.close()
     if pg is not None:
@@ -581,6 +704,8 @@ def main():
     ap.add_argument("--isec-only", action="store_true",
                     help="only the intersection-only batch (1M triangles, 16M rays)")
     ap.add_argument("--isec-rays", type=int, default=0)
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the Cornell and intersection-only workloads after the headline")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default engine configuration (profiling runs)")
     ap.add_argument("--slots", type=int, default=0, help="engine queue slots with --no-autotune")

@@ -125,8 +125,35 @@ typedef struct SnogRenderParams {
   float bg_alpha;            /* [background_alpha], default 1 */
   uint64_t seed;             /* stream selector for the GPU's counter-based RNG */
   uint32_t integrator;       /* [surface_integ.type]: SNOG_INTEG_PATH or SNOG_INTEG_DIRECT */
-  uint32_t reserved;         /* 0 */
+  uint32_t flags;            /* SNOG_RENDER_* bits, 0 by default */
 } SnogRenderParams;
+
+/* SnogRenderParams::flags.  COUNT_TRAVERSAL: the path integrator's traversal
+ * kernels count their node visits and primitive tests into SnogRenderStats
+ * (closest_nodes ...), the counts behind the reference's
+ * RenderStats::IsecStats (render/render-stats.h:30-52); it costs one
+ * warp-reduced atomic per warp per launch. */
+enum { SNOG_RENDER_COUNT_TRAVERSAL = 1 };
+
+/* The pixels to render and the output window of a partial render, as the
+ * reference's --limit option sets them up (snogray.lua:442-454, 543-550).
+ * The film is params->width x params->height pixels (the RenderMgr's size,
+ * render-mgr/render-mgr.h:39-40); film pixel (0, 0) is the top-left one.
+ *   pattern: the film rectangle [pat_x, pat_x + pat_width) x
+ *            [pat_y, pat_y + pat_height) whose pixels get samples
+ *            (RenderPattern (left_x, top_y, width, height),
+ *            render-mgr/render-pattern.h:105-108); it may extend beyond the
+ *            film, as the filter margin does;
+ *   output:  out_width x out_height pixels whose top-left is film pixel
+ *            (out_x, out_y) (ImageSampledOutput's sample_base_x/y and size,
+ *            snogray.lua:451-454).
+ * Every sample adds to the output pixels its Mitchell filter reaches. */
+typedef struct SnogRenderWindow {
+  int32_t pat_x, pat_y;
+  uint32_t pat_width, pat_height;
+  int32_t out_x, out_y;
+  uint32_t out_width, out_height;
+} SnogRenderWindow;
 
 /* Surface integrators: PathInteg (render/path-integ.cc:134-407) and
  * DirectInteg, direct lighting plus specular recursion with roulette beyond
@@ -157,10 +184,18 @@ typedef struct SnogRenderStats {
   uint32_t kernel_launches;
   /* Filled only when the environment variable SNOG_PROFILE_KERNELS=1: device
    * time of each kernel kind summed over its launches (CUDA events on the
-   * render stream), and the traversal's node visits / primitive tests. */
+   * render stream). */
   double closest_ms, shadow_ms, shade_ms, other_ms;
   uint32_t closest_launches, shadow_launches;
+  /* Node visits and primitive tests of the closest-hit and shadow queries
+   * (space_node_intersect_calls and surface_intersects_tests of the
+   * reference's IsecStats, without its negative cache), filled by the path
+   * integrator when params->flags has SNOG_RENDER_COUNT_TRAVERSAL or
+   * SNOG_PROFILE_KERNELS=1. */
   uint64_t closest_nodes, closest_tests, shadow_nodes, shadow_tests;
+  /* Vertices lit by direct illumination (the reference's
+   * RenderStats::illum_calls), path integrator. */
+  uint64_t illum_calls;
 } SnogRenderStats;
 
 typedef struct SnogScene SnogScene;
@@ -260,6 +295,15 @@ int snog_render(SnogScene *scene, const SnogCamera *camera, const SnogRenderPara
 int snog_render_device(SnogScene *scene, const SnogCamera *camera,
                        const SnogRenderParams *params, float *d_out_rgb, void *stream,
                        SnogRenderStats *stats);
+
+/* Render the pattern of WINDOW into its output window (HOST memory out_rgb:
+ * window->out_height rows of window->out_width RGB floats, top row first).
+ * Replaces RenderMgr::render (unsigned num_threads, RenderPattern &,
+ * ImageSampledOutput &, Progress &, RenderStats &)
+ * (render-mgr/render-mgr.h:45-50, render-mgr.cc:50-74) for partial renders;
+ * WINDOW NULL is snog_render.  stats->paths counts the pattern's samples. */
+int snog_render_window(SnogScene *scene, const SnogCamera *camera, const SnogRenderParams *params,
+                       const SnogRenderWindow *window, float *out_rgb, SnogRenderStats *stats);
 
 /* ---- Batched and served rendering ---------------------------------------
  * The streaming engine traces many jobs (scene, camera, size, samples) in one
@@ -374,8 +418,9 @@ int snog_server_destroy(SnogServer *server);
  * device mid-loop.  Limits: at most 1048576 output pixels, and a wave of the
  * scratch must hold one pixel's samples; larger jobs return SNOG_EINVAL.  The
  * first call on a device looks up the array's address and should come before
- * any stream capture.  Calls share the array: calls whose work overlaps on
- * the GPU race and must be ordered by the caller (e.g. one stream). */
+ * any stream capture.  The scene's device must be the current device
+ * (SNOG_EINVAL otherwise).  Calls share the array: calls whose work overlaps
+ * on the GPU race and must be ordered by the caller (e.g. one stream). */
 int snog_render_device_noalloc(SnogScene *scene, const SnogCamera *camera,
                                const SnogRenderParams *params, float *d_out_rgb, void *stream);
 

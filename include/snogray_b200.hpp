@@ -27,8 +27,13 @@
 //   SurfaceGroup::add (surface | light)          surface/surface-group.h:36-40
 //   Camera: move, point, set_vert_fov, set_horiz_fov  camera/camera.h:84-128, 231-247
 //   GlobalRenderState (scene, params)            render/global-render-state.cc:28-49
-//   RenderMgr (state, camera, w, h); render (output, stats)  render-mgr/render-mgr.h:39-50
-//   ImageSampledOutput               image/image-sampled-output.h
+//   RenderMgr (state, camera, w, h); render (num_threads, pattern, output,
+//                                    progress, stats)  render-mgr/render-mgr.h:39-50
+//   RenderPattern (left_x, top_y, width, height)  render-mgr/render-pattern.h:105-108
+//   Progress (set_start, set_size, start, update, end)  util/progress.h
+//   RenderStats, RenderStats::IsecStats  render/render-stats.h:24-71
+//   ImageSampledOutput (w, h [, sample_base_x, sample_base_y])
+//                                    image/image-sampled-output.h:54-56
 //
 // Differences: one CUDA device per process (snog_init); surfaces are owned by
 // shared pointers rather than the reference's raw-pointer ownership by the
@@ -567,10 +572,18 @@ class Camera {
 };
 
 // The finished image: HEIGHT rows of WIDTH RGB floats, top row first (the
-// flushed values of the reference's ImageSampledOutput).
+// flushed values of the reference's ImageSampledOutput).  Its top-left pixel
+// is film pixel (sample_base_x, sample_base_y), the offset a --limit render
+// gives its output (snogray.lua:451-452); 0, 0 for a whole image.
 class ImageSampledOutput {
  public:
-  ImageSampledOutput(uint32_t w, uint32_t h) : width(w), height(h), rgb(size_t(w) * h * 3) {}
+  ImageSampledOutput(uint32_t w, uint32_t h, int32_t base_x = 0, int32_t base_y = 0)
+      : width(w), height(h), sample_base_x(base_x), sample_base_y(base_y), rgb(size_t(w) * h * 3) {}
+  // The Mitchell filter's reach in pixels, the margin the reference's driver
+  // adds around a render pattern (image/image-filter-conv.h:39-40,
+  // snogray.lua:543-550).
+  int filter_x_radius() const { return 2; }
+  int filter_y_radius() const { return 2; }
   // Portable float map (little-endian), bottom row first as PFM stores it.
   void write_pfm(const std::string &path) const {
     FILE *f = std::fopen(path.c_str(), "wb");
@@ -580,23 +593,112 @@ class ImageSampledOutput {
     std::fclose(f);
   }
   uint32_t width, height;
+  int32_t sample_base_x, sample_base_y;
   std::vector<float> rgb;
 };
 
+// The pixels to render: the film rectangle [left_x, left_x + width) x
+// [top_y, top_y + height) (render-mgr/render-pattern.h:105-108).
+class RenderPattern {
+ public:
+  RenderPattern(int left_x, int top_y, int width, int height)
+      : x_beg(left_x), y_beg(top_y), x_end(left_x + width), y_end(top_y + height) {}
+  int left_x() const { return x_beg; }
+  int top_y() const { return y_beg; }
+  int width() const { return x_end - x_beg; }
+  int height() const { return y_end - y_beg; }
+
+ private:
+  int x_beg, y_beg, x_end, y_end;
+};
+
+// Progress reports (util/progress.h): the render calls set_start and
+// set_size with the pattern's position range, start, one update at the end
+// of the device work, and end.
+class Progress {
+ public:
+  virtual ~Progress() = default;
+  virtual void set_start(int) {}
+  virtual void set_size(unsigned) {}
+  virtual void start() {}
+  virtual void update(int) {}
+  virtual void end() {}
+};
+
+// The reference's render statistics (render/render-stats.h:24-71):
+// scene_intersect_calls and scene_shadow_tests count closest-hit and shadow
+// queries; IsecStats counts the traversal's node visits and primitive tests
+// (the path integrator's; the negative cache the reference keeps is not used
+// here, so neg_cache_* stay 0 and a primitive met twice by one ray is tested
+// twice).  illum_calls counts vertices lit (path integrator).  paths and
+// device_ms are this library's additions.
 struct RenderStats {
-  uint64_t paths = 0, closest_rays = 0, shadow_rays = 0;
+  struct IsecStats {
+    unsigned long long surface_intersects_tests = 0, surface_intersects_hits = 0;
+    unsigned long long neg_cache_hits = 0, neg_cache_collisions = 0;
+    unsigned long long space_node_intersect_calls = 0;
+  };
+  unsigned long long scene_intersect_calls = 0, scene_shadow_tests = 0, illum_calls = 0;
+  IsecStats intersect, shadow;
+  uint64_t paths = 0;
   double device_ms = 0;
+  // Names this library used before the reference's fields were added.
+  uint64_t closest_rays = 0, shadow_rays = 0;
 };
 
 class RenderMgr {
  public:
   RenderMgr(const GlobalRenderState &state, const Camera &camera, unsigned width, unsigned height)
       : state_(state), camera_(camera), width_(width), height_(height) {}
-  // Render the whole image into OUTPUT (whose size must match).
+
+  // Render the pixels of PATTERN into OUTPUT, as the reference's
+  // RenderMgr::render (render-mgr/render-mgr.h:45-50): the film is the
+  // renderer's width x height, OUTPUT covers the film pixels from its
+  // sample base, and every sample adds to the output pixels its filter
+  // reaches.  NUM_THREADS is accepted for the signature's sake: the work runs
+  // on the GPU.  STATS is added to, as the reference's is.
+  void render(unsigned num_threads, RenderPattern &pattern, ImageSampledOutput &output, Progress &prog,
+              RenderStats &stats) {
+    (void)num_threads;
+    SnogRenderWindow win{};
+    win.pat_x = pattern.left_x();
+    win.pat_y = pattern.top_y();
+    if (pattern.width() <= 0 || pattern.height() <= 0)
+      throw std::runtime_error("RenderMgr::render: empty render pattern");
+    win.pat_width = uint32_t(pattern.width());
+    win.pat_height = uint32_t(pattern.height());
+    win.out_x = output.sample_base_x;
+    win.out_y = output.sample_base_y;
+    win.out_width = output.width;
+    win.out_height = output.height;
+    const SnogCamera cam = camera_.c_struct();
+    SnogRenderParams p = params();
+    p.flags |= SNOG_RENDER_COUNT_TRAVERSAL;
+    const unsigned npos = unsigned(pattern.width()) * unsigned(pattern.height());
+    prog.set_start(0);
+    prog.set_size(npos);
+    prog.start();
+    SnogRenderStats st{};
+    check(snog_render_window(state_.handle(), &cam, &p, &win, output.rgb.data(), &st), "RenderMgr::render");
+    prog.update(int(npos));
+    prog.end();
+    add(stats, st);
+  }
+
+  // The whole image (the pattern with the filter margin, snogray.lua:543-550)
+  // into OUTPUT, whose size must be the renderer's.
   void render(ImageSampledOutput &output, RenderStats &stats) {
     if (output.width != width_ || output.height != height_)
       throw std::runtime_error("RenderMgr::render: output size differs from the renderer's");
     const SnogCamera cam = camera_.c_struct();
+    SnogRenderParams p = params();
+    SnogRenderStats st{};
+    check(snog_render(state_.handle(), &cam, &p, output.rgb.data(), &st), "RenderMgr::render");
+    add(stats, st);
+  }
+
+ private:
+  SnogRenderParams params() const {
     SnogRenderParams p{};
     p.width = width_;
     p.height = height_;
@@ -609,15 +711,22 @@ class RenderMgr {
     p.min_trace = state_.params.min_trace;
     p.bg_alpha = state_.params.background_alpha;
     p.seed = state_.params.seed;
-    SnogRenderStats st{};
-    check(snog_render(state_.handle(), &cam, &p, output.rgb.data(), &st), "RenderMgr::render");
+    return p;
+  }
+  static void add(RenderStats &stats, const SnogRenderStats &st) {
+    stats.scene_intersect_calls += st.closest_rays;
+    stats.scene_shadow_tests += st.shadow_rays;
+    stats.intersect.space_node_intersect_calls += st.closest_nodes;
+    stats.intersect.surface_intersects_tests += st.closest_tests;
+    stats.shadow.space_node_intersect_calls += st.shadow_nodes;
+    stats.shadow.surface_intersects_tests += st.shadow_tests;
+    stats.illum_calls += st.illum_calls;
     stats.paths += st.paths;
     stats.closest_rays += st.closest_rays;
     stats.shadow_rays += st.shadow_rays;
     stats.device_ms += st.device_ms;
   }
 
- private:
   const GlobalRenderState &state_;
   Camera camera_;
   unsigned width_, height_;

@@ -18,10 +18,12 @@
 //                                   (load/mesh/load-ply.cc) and dump its
 //                                   vertices, normals and triangles; a load
 //                                   error is written to OUT as its message
-//   render SPEC OUT.pfm [threads] [seed_skip] [spp] [row0] [rows] [repeat]
+//   render SPEC OUT.pfm [threads] [seed_skip] [spp] [row0] [rows] [repeat] [keep]
 //                                   RenderMgr::render of the whole image
 //                                   (render-mgr/render-mgr.cc:50-74), or of
-//                                   a band of rows for a bounded CPU sample
+//                                   a band of rows for a bounded CPU sample;
+//                                   with KEEP nonzero, repetition r writes
+//                                   OUT.pfm.r.pfm instead of overwriting OUT.pfm
 //
 // The reference keeps octree nodes, surface lists and camera fields private;
 // this program (and only this program) reads them by compiling the
@@ -364,7 +366,8 @@ int mode_trace(const std::string &spec, const std::string &rays_path, const std:
 }
 
 int mode_render(const std::string &spec, const std::string &out, unsigned threads,
-                unsigned seed_skip, unsigned spp_override, int row0, int rows, unsigned repeat) {
+                unsigned seed_skip, unsigned spp_override, int row0, int rows, unsigned repeat,
+                bool keep) {
   RefScene rs;
   snogspec::Scene peek = snogspec::load(spec);
   (void)peek;
@@ -398,7 +401,7 @@ int mode_render(const std::string &spec, const std::string &out, unsigned thread
   // output; the scene (and its octree) is built once.
   for (unsigned rep = 0; rep < repeat; rep++) {
     ValTable out_params;
-    ImageSampledOutput output(out, w, hgt, out_params);
+    ImageSampledOutput output(keep ? out + "." + std::to_string(rep) + ".pfm" : out, w, hgt, out_params);
     int xm = int(output.filter_x_radius()), ym = int(output.filter_y_radius());
     RenderPattern pattern(0 - xm, y0 - ym, int(w) + 2 * xm, nrows + 2 * ym);
     RenderMgr mgr(*rs.grs, camera, w, hgt);
@@ -476,7 +479,7 @@ int main(int argc, char **argv) {
       return mode_render(argv[2], argv[3], argc > 4 ? atoi(argv[4]) : 1,
                          argc > 5 ? atoi(argv[5]) : 0, argc > 6 ? atoi(argv[6]) : 0,
                          argc > 7 ? atoi(argv[7]) : 0, argc > 8 ? atoi(argv[8]) : 0,
-                         argc > 9 ? unsigned(atoi(argv[9])) : 1u);
+                         argc > 9 ? unsigned(atoi(argv[9])) : 1u, argc > 10 && atoi(argv[10]) != 0);
     throw std::runtime_error("bad arguments");
   } catch (std::exception &e) {
     fprintf(stderr, "snog_ref: %s\n", e.what());

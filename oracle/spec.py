@@ -18,7 +18,26 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_TREE = "/root/reference"
+# The reference source tree; SNOGRAY_REFERENCE overrides the default location.
+REFERENCE_TREE = os.environ.get("SNOGRAY_REFERENCE", "/root/reference")
+
+
+def _scenes_module():
+    """snogray_b200/scenes.py (numpy only) without importing the package,
+    whose __init__ maps the CUDA library."""
+    import importlib.util
+    import sys
+    name = "snogray_b200.scenes"
+    if name in sys.modules:
+        return sys.modules[name]
+    if "_snog_scenes_file" in sys.modules:
+        return sys.modules["_snog_scenes_file"]
+    path = os.path.join(os.path.dirname(HERE), "snogray_b200", "scenes.py")
+    spec_ = importlib.util.spec_from_file_location("_snog_scenes_file", path)
+    mod = importlib.util.module_from_spec(spec_)
+    sys.modules["_snog_scenes_file"] = mod
+    spec_.loader.exec_module(mod)
+    return mod
 
 
 def ref_binary(flavour="parity"):
@@ -40,7 +59,8 @@ def build(targets=("all",), quiet=True):
     tg = list(targets)
     if "all" in tg and not os.path.isdir(REFERENCE_TREE):
         tg = ["port"]
-    out = subprocess.run(["make", "-C", HERE, "-j8", *tg], capture_output=True, text=True)
+    out = subprocess.run(["make", "-C", HERE, "-j8", f"REF={REFERENCE_TREE}", *tg], capture_output=True,
+                         text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
     return out
@@ -53,10 +73,12 @@ def ensure_port():
 
 
 def write_spec(path, scene, camera=None, params=None):
-    """Write SCENE (snogray_b200.scenes.SceneData) with CAMERA and PARAMS."""
-    from snogray_b200.scenes import RenderParams, Camera
-    params = params or RenderParams()
-    camera = camera or Camera()
+    """Write SCENE (snogray_b200.scenes.SceneData) with CAMERA and PARAMS.
+    The scene module is loaded from its file, so writing a spec never loads
+    the product's CUDA library."""
+    sc = _scenes_module()
+    params = params or sc.RenderParams()
+    camera = camera or sc.Camera()
     env = scene.envmap
     env_h, env_w = (env.shape[0], env.shape[1]) if env is not None else (0, 0)
     hdr = bytearray()
@@ -189,6 +211,25 @@ def ref_render(scene, camera, params, threads=1, seed_skip=0, spp=0, row0=0, row
                      str(spp), str(row0), str(rows)], timeout=timeout)
         img = read_pfm(op)
     return img, info
+
+
+def ref_render_repeat(scene, camera, params, repeat, threads=8, spp=0, flavour="parity", tmpdir=None,
+                      timeout=7200, reduce=None):
+    """REPEAT independent renders of one job in one reference process (the
+    scene and its octree are built once; every render's RenderContexts draw
+    fresh seeds).  Returns ([reduce(image) for each render], [info per
+    render]); REDUCE defaults to the identity."""
+    reduce = reduce or (lambda im: im)
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, op = os.path.join(d, "s.spec"), os.path.join(d, "o.pfm")
+        write_spec(sp, scene, camera, params)
+        out = subprocess.run([ref_binary(flavour), "render", sp, op, str(threads), "0", str(spp), "0", "0",
+                              str(repeat), "1"], capture_output=True, text=True, timeout=timeout)
+        if out.returncode != 0:
+            raise RuntimeError(f"reference render failed ({out.returncode}): {out.stderr[-2000:]}")
+        infos = [json.loads(ln) for ln in out.stdout.splitlines() if ln.startswith("{")]
+        outs = [reduce(read_pfm(f"{op}.{r}.pfm")) for r in range(repeat)]
+    return outs, infos
 
 
 def port_trace(scene, soa, n_closest, threads=8, tmpdir=None):

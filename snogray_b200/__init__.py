@@ -73,7 +73,16 @@ class SnogRenderParams(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
                 ("min_path_len", C.c_uint32), ("max_path_len", C.c_uint32),
                 ("direct_samples", C.c_uint32), ("min_trace", C.c_float), ("bg_alpha", C.c_float),
-                ("seed", C.c_uint64), ("integrator", C.c_uint32), ("reserved", C.c_uint32)]
+                ("seed", C.c_uint64), ("integrator", C.c_uint32), ("flags", C.c_uint32)]
+
+
+SNOG_RENDER_COUNT_TRAVERSAL = 1
+
+
+class SnogRenderWindow(C.Structure):
+    _fields_ = [("pat_x", C.c_int32), ("pat_y", C.c_int32), ("pat_width", C.c_uint32),
+                ("pat_height", C.c_uint32), ("out_x", C.c_int32), ("out_y", C.c_int32),
+                ("out_width", C.c_uint32), ("out_height", C.c_uint32)]
 
 
 class SnogSceneInfo(C.Structure):
@@ -92,7 +101,7 @@ class SnogRenderStats(C.Structure):
                 ("other_ms", C.c_double), ("closest_launches", C.c_uint32),
                 ("shadow_launches", C.c_uint32), ("closest_nodes", C.c_uint64),
                 ("closest_tests", C.c_uint64), ("shadow_nodes", C.c_uint64),
-                ("shadow_tests", C.c_uint64)]
+                ("shadow_tests", C.c_uint64), ("illum_calls", C.c_uint64)]
 
 
 class SnogEngineConfig(C.Structure):
@@ -141,6 +150,8 @@ _render = _sig("snog_render", C.c_int, _P, C.POINTER(SnogCamera), C.POINTER(Snog
                C.POINTER(SnogRenderStats))
 _render_device = _sig("snog_render_device", C.c_int, _P, C.POINTER(SnogCamera),
                       C.POINTER(SnogRenderParams), _P, _P, C.POINTER(SnogRenderStats))
+_render_window = _sig("snog_render_window", C.c_int, _P, C.POINTER(SnogCamera), C.POINTER(SnogRenderParams),
+                      C.POINTER(SnogRenderWindow), _P, C.POINTER(SnogRenderStats))
 
 
 _engine_default = _sig("snog_engine_default_config", C.c_int, C.POINTER(SnogEngineConfig))
@@ -199,7 +210,8 @@ def camera_struct(cam: Camera) -> SnogCamera:
 
 def params_struct(p: RenderParams) -> SnogRenderParams:
     return SnogRenderParams(p.width, p.height, p.spp, p.min_path_len, p.max_path_len,
-                            p.direct_samples, p.min_trace, p.bg_alpha, p.seed, p.integrator, 0)
+                            p.direct_samples, p.min_trace, p.bg_alpha, p.seed, p.integrator,
+                            getattr(p, "flags", 0))
 
 
 class Scene:
@@ -317,6 +329,20 @@ class Scene:
         st = SnogRenderStats()
         cs, ps = camera_struct(camera), params_struct(params)
         _check(_render(self._h, C.byref(cs), C.byref(ps), _ptr(out), C.byref(st)))
+        return out, {f: getattr(st, f) for f, _ in SnogRenderStats._fields_}
+
+    def render_window(self, camera: Camera, params: RenderParams, pattern, output):
+        """Render the film rectangle PATTERN = (left_x, top_y, width, height)
+        into the output window OUTPUT = (base_x, base_y, width, height) of
+        the params.width x params.height film (the reference's
+        RenderMgr::render with a RenderPattern and a sample-based
+        ImageSampledOutput).  Returns ((out_h, out_w, 3) image, stats)."""
+        win = SnogRenderWindow(int(pattern[0]), int(pattern[1]), int(pattern[2]), int(pattern[3]),
+                               int(output[0]), int(output[1]), int(output[2]), int(output[3]))
+        out = np.empty((int(output[3]), int(output[2]), 3), np.float32)
+        st = SnogRenderStats()
+        cs, ps = camera_struct(camera), params_struct(params)
+        _check(_render_window(self._h, C.byref(cs), C.byref(ps), C.byref(win), _ptr(out), C.byref(st)))
         return out, {f: getattr(st, f) for f, _ in SnogRenderStats._fields_}
 
     def render_device(self, camera: Camera, params: RenderParams, d_out, stream=None,

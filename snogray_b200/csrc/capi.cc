@@ -136,10 +136,12 @@ RenderPool &render_pool(int device) {
 // Render with the device's pooled working memory; the resolved image goes to
 // d_out (device) or, if null, to h_out (host, copied before returning).
 static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
-                        float *h_out, cudaStream_t st, SnogRenderStats *stats) {
+                        float *h_out, cudaStream_t st, SnogRenderStats *stats,
+                        const SnogRenderWindow *win = nullptr) {
   check_params(p);
+  if (win) check_window(p, *win);
   if (p.integrator == SNOG_INTEG_DIRECT) {   // the streaming engine carries its spawned rays
-    render_on_engine(S, cam, p, d_out, h_out, st, stats);
+    render_on_engine(S, cam, p, d_out, h_out, st, stats, win);
     return;
   }
   if (!stack_class_for_depth(S.dev.max_depth))
@@ -148,11 +150,12 @@ static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderPar
   std::lock_guard<std::mutex> plk(pool.mu);
   if (!pool.done) check_cuda(cudaEventCreateWithFlags(&pool.done, cudaEventDisableTiming), "event");
   RenderCache &rc = pool.rc;
-  const uint64_t total = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
+  JobConsts jc = make_job(S.dev, cam, p, win);
+  const uint64_t total = job_total(jc);
   // Shadow-queue entries a vertex may need: two per light sample.
   const uint32_t ls = std::max(1u, S.dev.n_lights) * std::max(1u, p.direct_samples);
   uint64_t cap = choose_wave_cap(total, p.spp, ls);
-  const size_t npix = size_t(p.width) * p.height;
+  const size_t npix = size_t(jc.W) * jc.H;
   const bool grow = rc.wb.wave_cap < cap || rc.wb.n_lights < ls || rc.npix_cap < npix;
   // Buffers about to be replaced may still be in use by a render on another stream.
   if (grow) check_cuda(cudaEventSynchronize(pool.done), "pool wait");
@@ -177,7 +180,6 @@ static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderPar
     check_cuda(cudaMalloc(&rc.out, npix * 3 * sizeof(float)), "out");
     rc.npix_cap = npix;
   }
-  JobConsts jc = make_job(S.dev, cam, p);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (stats) {
     check_cuda(cudaEventCreate(&e0), "event");
@@ -187,11 +189,12 @@ static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderPar
   uint32_t waves = 0, launches = 0;
   const char *pe = getenv("SNOG_PROFILE_KERNELS");
   const bool profile = stats && pe && pe[0] == '1';
+  const bool count = stats && (profile || (p.flags & SNOG_RENDER_COUNT_TRAVERSAL));
   RenderProfile prof;
   WaveBuffers wave = rc.wb;   // the pool may be larger than this job's wave
   wave.wave_cap = cap;
   cudaError_t e = render_job(S.dev, jc, wave, rc.accum, rc.wsum, d_out ? d_out : rc.out, st, &waves,
-                             &launches, profile ? &prof : nullptr);
+                             &launches, profile ? &prof : nullptr, count);
   if (e == cudaSuccess && !d_out)
     e = cudaMemcpyAsync(h_out, rc.out, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaEventRecord(pool.done, st);
@@ -208,17 +211,18 @@ static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderPar
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    unsigned long long hs[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long hs[7] = {0, 0, 0, 0, 0, 0, 0};
     uint32_t flags[4] = {0, 0, 0, 0};
-    check_cuda(cudaMemcpy(hs, rc.wb.stats, 48, cudaMemcpyDeviceToHost), "stats");
+    check_cuda(cudaMemcpy(hs, rc.wb.stats, sizeof hs, cudaMemcpyDeviceToHost), "stats");
     check_cuda(cudaMemcpy(flags, rc.wb.counters, 16, cudaMemcpyDeviceToHost), "flags");
-    if (flags[3]) throw Error{SNOG_EINVAL, "traversal stack overflow (non-finite ray?)"};
+    check_render_flags(flags[3]);
     stats->paths = total;
     stats->closest_rays = hs[0];
     stats->shadow_rays = hs[1];
     stats->device_ms = ms;
     stats->waves = waves;
     stats->kernel_launches = launches;
+    stats->illum_calls = hs[6];
     if (profile) {
       check_cuda(prof.collect(), "profile events");
       stats->closest_ms = prof.ms[RenderProfile::CLOSEST];
@@ -227,6 +231,8 @@ static void render_into(SceneImpl &S, const SnogCamera &cam, const SnogRenderPar
       stats->other_ms = prof.ms[RenderProfile::OTHER];
       stats->closest_launches = prof.launches[RenderProfile::CLOSEST];
       stats->shadow_launches = prof.launches[RenderProfile::SHADOW];
+    }
+    if (count) {
       stats->closest_nodes = hs[2];
       stats->closest_tests = hs[3];
       stats->shadow_nodes = hs[4];
@@ -265,7 +271,19 @@ int snog_render_device(SnogScene *scene, const SnogCamera *camera, const SnogRen
   });
 }
 
-const char *snog_version(void) { return "snogray_b200 0.1 (sm_100a)"; }
+int snog_render_window(SnogScene *scene, const SnogCamera *camera, const SnogRenderParams *params,
+                       const SnogRenderWindow *window, float *out_rgb, SnogRenderStats *stats) {
+  return guarded([&] {
+    if (!scene || !camera || !params || !out_rgb) throw Error{SNOG_EINVAL, "null argument"};
+    SceneImpl &S = *scene->impl;
+    if (!S.on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
+    std::lock_guard<std::mutex> lk(S.mu);
+    render_into(S, *camera, *params, nullptr, out_rgb, nullptr, stats, window);
+    return int(SNOG_OK);
+  });
+}
+
+const char *snog_version(void) { return "snogray_b200 0.2 (sm_100a)"; }
 
 const char *snog_last_error(void) { return g_last_error.c_str(); }
 

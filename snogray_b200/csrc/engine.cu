@@ -107,12 +107,12 @@ __global__ void __launch_bounds__(256) k_e_regen(EngineCtl *ctl, const WorkItem 
     const EngineJobDev &J = jobs[job];
     const JobConsts &jc = J.jc;
     const uint32_t pixel = uint32_t(g / jc.S), s = uint32_t(g % jc.S);
-    const int px = int(pixel % jc.PW) - 2, py = int(pixel / jc.PW) - 2;
+    const int px = jc.PX + int(pixel % jc.PW), py = jc.PY + int(pixel / jc.PW);
     Rng rng{jc.seed_lo, jc.seed_hi, uint32_t(g), uint32_t(g >> 32)};
     const float2 j = strat_uv(strata_for(jc.S), rng, pixel, s, dim_of(0, K_CAMERA));
     // Renderer::render_packet (render-mgr/renderer.cc:69-88), Camera::eye_vec (camera/camera.h:384-389)
     const float cu = float(px) + j.x, cv = float(py) + j.y;
-    const float fu = cu / float(jc.W), fv = (float(jc.H) - cv) / float(jc.H);
+    const float fu = cu / float(jc.FW), fv = (float(jc.FH) - cv) / float(jc.FH);
     const float x = 2.f * fu - 1.f, y = 2.f * fv - 1.f;
     const float3 d = add(add(load3(jc.cam_fwd), mul(mul(load3(jc.cam_right), x), jc.tan_x)),
                          mul(mul(load3(jc.cam_up), y), jc.tan_y));
@@ -313,7 +313,12 @@ __global__ void __launch_bounds__(128, SNOG_SHADE_MINBLOCKS) k_e_shade(EngineCtl
         uint32_t nps = (ps & ~0x1ffu) | (bounce + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
         if (bs.flags & B_TRANSMISSIVE) {
           const uint32_t mid = s->mats[I.mat].medium_id;
-          if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
+          if (mid && I.back) {
+            nps = ps_pop(nps);
+          } else if (mid && !ps_push(nps, mid)) {
+            atomicOr(&ctl->err, 2u);   // a fifth nested medium: the path ends here
+            continue;
+          }
         }
         if (!cont) {
           cont = true;
@@ -795,28 +800,33 @@ uint64_t Engine::scene_check(uint32_t scene_slot) const {
 }
 
 uint64_t Engine::submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRenderParams &p, float *out,
-                        bool out_on_device, double submit_ms, Checkpoint *resume) {
+                        bool out_on_device, double submit_ms, Checkpoint *resume, const SnogRenderWindow *win) {
   if (scene_slot >= scenes_.size()) throw Error{SNOG_ENOTFOUND, "unknown scene slot"};
   if (p.width == 0 || p.height == 0 || p.spp == 0) throw Error{SNOG_EINVAL, "width, height, spp must be > 0"};
   if (p.max_path_len > 255) throw Error{SNOG_EINVAL, "max_path_len must be <= 255"};
   if (p.integrator > SNOG_INTEG_DIRECT) throw Error{SNOG_EINVAL, "unknown integrator"};
   if (p.direct_samples > 64) throw Error{SNOG_EINVAL, "direct_samples must be <= 64"};
-  if (uint64_t(p.width + 4) * (p.height + 4) * p.spp >= (1ull << 32))
-    throw Error{SNOG_EINVAL, "a job is limited to 2^32 paths"};
+  if (win) {
+    check_window(p, *win);
+    if (resume) throw Error{SNOG_EINVAL, "a windowed job cannot resume a checkpoint"};
+  }
+  const uint64_t pat_pixels =
+      win ? uint64_t(win->pat_width) * win->pat_height : uint64_t(p.width + 4) * (p.height + 4);
+  if (pat_pixels * p.spp >= (1ull << 32)) throw Error{SNOG_EINVAL, "a job is limited to 2^32 paths"};
   if (scenes_[scene_slot]->dev.n_lights * p.direct_samples > cfg_.max_lights)
     throw Error{SNOG_EINVAL, "lights x direct_samples exceeds the engine's max_lights"};
   HostJob j;
   j.id = next_id_++;
   j.scene_slot = scene_slot;
-  j.jc = make_job(scenes_[scene_slot]->dev, cam, p);
-  j.total = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
-  j.npix = size_t(p.width) * p.height;
+  j.jc = make_job(scenes_[scene_slot]->dev, cam, p, win);
+  j.total = job_total(j.jc);
+  j.npix = size_t(j.jc.W) * j.jc.H;
   j.out = out;
   j.out_on_device = out_on_device;
   j.bytes = j.total * 24 + j.npix * (20 + (out_on_device ? 0 : 12)) + 4096;
   if (j.bytes > cfg_.mem_budget) throw Error{SNOG_ENOMEM, "job larger than the engine's memory budget"};
   j.st.submit_ms = submit_ms >= 0 ? submit_ms : now_ms();
-  j.st.paths = uint64_t(p.width) * p.height * p.spp;
+  j.st.paths = uint64_t(j.jc.W) * j.jc.H * p.spp;
   j.cam = cam;
   j.params = p;
   if (resume) {
@@ -1091,7 +1101,7 @@ bool Engine::step() {
     check_cuda(cudaStreamSynchronize(stream_), "iteration");
     staging_used_ = 0;
     last_ctl_ = *ctl_host_;
-    if (last_ctl_.err) throw Error{SNOG_EINVAL, "traversal stack overflow (non-finite ray?)"};
+    check_render_flags(last_ctl_.err);
     if (profile_on_) {
       for (uint32_t it = 0; it < 2 * cfg_.iters_per_launch; it++) {
         const cudaEvent_t *ev = &events_[5 * it];

@@ -146,8 +146,11 @@ class Engine {
   // SUBMIT_MS (engine clock) overrides the submission time recorded.
   // RESUME (optional): continue from a checkpoint of the same camera and
   // parameters on the same scene; its paths are not traced again.
+  // WIN (may be null) renders a pattern into an output window (make_job);
+  // such a job cannot be resumed from a checkpoint.
   uint64_t submit(uint32_t scene_slot, const SnogCamera &cam, const SnogRenderParams &p, float *out,
-                  bool out_on_device, double submit_ms = -1, Checkpoint *resume = nullptr);
+                  bool out_on_device, double submit_ms = -1, Checkpoint *resume = nullptr,
+                  const SnogRenderWindow *win = nullptr);
   bool cancel(uint64_t job);
   // Stop (PAUSE) or restart pushing a job's work; paths already pushed finish.
   bool pause(uint64_t job, bool pause);

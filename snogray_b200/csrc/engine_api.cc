@@ -34,7 +34,7 @@ using namespace snog;
 namespace snog {
 
 void render_on_engine(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
-                      float *h_out, cudaStream_t st, SnogRenderStats *stats) {
+                      float *h_out, cudaStream_t st, SnogRenderStats *stats, const SnogRenderWindow *win) {
   static std::mutex mu;
   static std::map<int, std::unique_ptr<Engine>> engines;
   std::lock_guard<std::mutex> lk(mu);
@@ -56,13 +56,14 @@ void render_on_engine(SceneImpl &S, const SnogCamera &cam, const SnogRenderParam
   const uint32_t slot = e->add_scene(&S);
   e->clear_counters();
   const auto t0 = std::chrono::steady_clock::now();
-  const uint64_t id = e->submit(slot, cam, p, d_out ? d_out : h_out, d_out != nullptr);
+  const uint64_t id = e->submit(slot, cam, p, d_out ? d_out : h_out, d_out != nullptr, -1, nullptr, win);
   e->run_to_completion();
   const JobStatsHost js = e->stats(id);
   if (js.status != SNOG_OK) throw Error{js.status, "render did not complete"};
   if (stats) {
     std::memset(stats, 0, sizeof *stats);
-    stats->paths = uint64_t(p.width + 4) * (p.height + 4) * p.spp;
+    stats->paths = win ? uint64_t(win->pat_width) * win->pat_height * p.spp
+                       : uint64_t(p.width + 4) * (p.height + 4) * p.spp;
     stats->closest_rays = e->rays_closest();
     stats->shadow_rays = e->rays_shadow();
     stats->device_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -559,6 +560,16 @@ static Engine::Checkpoint read_checkpoint(const char *path) {
             std::fread(&c.cam, sizeof c.cam, 1, f) == 1 && std::fread(&c.params, sizeof c.params, 1, f) == 1 &&
             std::fread(&c.total, 8, 1, f) == 1 && std::fread(&c.done, 8, 1, f) == 1 &&
             std::fread(&c.scene_check, 8, 1, f) == 1 && c.done <= c.total && c.done <= (1ull << 32);
+  // The header is untrusted: its path counts must agree with the job's size
+  // and with the bytes that follow before anything is sized from them.
+  if (ok) ok = c.total == job_paths(c.params);
+  if (ok) {
+    const long here = std::ftell(f);
+    ok = here >= 0 && std::fseek(f, 0, SEEK_END) == 0;
+    const long end = ok ? std::ftell(f) : -1;
+    ok = ok && end >= here && uint64_t(end - here) == c.done * (sizeof(float4) + sizeof(float2)) &&
+         std::fseek(f, here, SEEK_SET) == 0;
+  }
   if (ok) {
     c.result.resize(c.done);
     c.jit.resize(c.done);

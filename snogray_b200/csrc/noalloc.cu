@@ -116,6 +116,13 @@ extern "C" int snog_render_device_noalloc(SnogScene *scene, const SnogCamera *ca
     if (!scene || !camera || !params || !d_out_rgb) throw Error{SNOG_EINVAL, "null argument"};
     SceneImpl &S = *scene->impl;
     if (!S.on_device) throw Error{SNOG_EINVAL, "scene was built host-only"};
+    // The scratch address and the scene's arrays must belong to one device:
+    // the scene's device has to be the current one.
+    int cur = -1;
+    check_cuda(cudaGetDevice(&cur), "cudaGetDevice");
+    if (cur != S.device)
+      throw Error{SNOG_EINVAL, "the scene was created on device " + std::to_string(S.device) +
+                                   " but device " + std::to_string(cur) + " is current"};
     const SnogRenderParams &p = *params;
     if (p.integrator != SNOG_INTEG_PATH)
       throw Error{SNOG_EINVAL, "the no-alloc render runs the path integrator only"};

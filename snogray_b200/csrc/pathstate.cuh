@@ -3,8 +3,8 @@
 // regeneration).
 //
 // A path's 32-bit state word holds its length (8 bits), the after-specular
-// flag (1 bit), the media-stack depth (2 bits) and up to three medium ids
-// (7 bits each).
+// flag (1 bit), the media-stack depth (3 bits) and up to four medium ids
+// (5 bits each: a scene has at most 31 distinct media besides the default).
 
 #ifndef SNOG_PATHSTATE_CUH
 #define SNOG_PATHSTATE_CUH
@@ -15,28 +15,27 @@ namespace snog {
 
 __device__ __forceinline__ uint32_t ps_len(uint32_t p) { return p & 0xffu; }
 __device__ __forceinline__ bool ps_spec(uint32_t p) { return (p >> 8) & 1u; }
-__device__ __forceinline__ uint32_t ps_depth(uint32_t p) { return (p >> 9) & 3u; }
-__device__ __forceinline__ uint32_t ps_medium(uint32_t p, uint32_t k) { return (p >> (11 + 7 * k)) & 0x7fu; }
+__device__ __forceinline__ uint32_t ps_depth(uint32_t p) { return (p >> 9) & 7u; }
+__device__ __forceinline__ uint32_t ps_medium(uint32_t p, uint32_t k) { return (p >> (12 + 5 * k)) & 0x1fu; }
+
+constexpr uint32_t kMediaStack = 4;   // media-stack entries in the path state word
 
 // Media::update_stack_for_transmission (material/media.cc:76-118): entering a
 // surface with a medium pushes it, leaving pops (never below the camera's
-// medium).  The stack holds three entries; a fourth push drops the oldest.
-__device__ __forceinline__ uint32_t ps_push(uint32_t p, uint32_t mid) {
-  uint32_t d = ps_depth(p);
-  uint32_t ids[3] = {ps_medium(p, 0), ps_medium(p, 1), ps_medium(p, 2)};
-  if (d == 3) {
-    ids[0] = ids[1];
-    ids[1] = ids[2];
-    d = 2;
-  }
-  ids[d] = mid & 0x7fu;
-  d++;
-  return (p & 0x1ffu) | (d << 9) | (ids[0] << 11) | (ids[1] << 18) | (ids[2] << 25);
+// medium).  The reference's stack is an unbounded list; this one holds four
+// entries, and a fifth push returns false (the caller ends the path and
+// reports the overflow as an error).
+__device__ __forceinline__ bool ps_push(uint32_t &p, uint32_t mid) {
+  const uint32_t d = ps_depth(p);
+  if (d >= kMediaStack) return false;
+  p = (p & ~(7u << 9)) | ((d + 1) << 9);
+  p = (p & ~(0x1fu << (12 + 5 * d))) | ((mid & 0x1fu) << (12 + 5 * d));
+  return true;
 }
 __device__ __forceinline__ uint32_t ps_pop(uint32_t p) {
   uint32_t d = ps_depth(p);
   if (d == 0) return p;
-  return (p & ~(3u << 9)) | ((d - 1) << 9);
+  return (p & ~(7u << 9)) | ((d - 1) << 9);
 }
 
 // RNG dimensions: vertex b, slot k.

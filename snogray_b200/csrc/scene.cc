@@ -23,6 +23,12 @@ void check_cuda(int err, const char *what) {
     throw Error{SNOG_ECUDA, std::string(what) + ": " + cudaGetErrorString(cudaError_t(err))};
 }
 
+void check_render_flags(uint32_t flags) {
+  if (flags & 1u) throw Error{SNOG_EINVAL, "traversal stack overflow (non-finite ray?)"};
+  if (flags & 2u)
+    throw Error{SNOG_EINVAL, "a path entered a fifth nested medium; the media stack holds four"};
+}
+
 void *DeviceArena::alloc(size_t n) {
   void *p = nullptr;
   size_t sz = n ? (n + 255) & ~size_t(255) : 256;
@@ -217,8 +223,19 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
       o.has_lambert = !(sum < 3 * 1e-15f);
     }
     if (m.type == SNOG_GLASS) {
-      o.medium_id = uint32_t(media.size());
-      media.push_back(DevMedium{m.ior_n, {m.absorb[0], m.absorb[1], m.absorb[2]}});
+      // A medium is its ior and absorption (material/medium.h:23-58), so
+      // glass materials with equal ones share a medium id.  The path state
+      // holds 5-bit ids: at most 31 distinct media besides the default.
+      const DevMedium md{m.ior_n, {m.absorb[0], m.absorb[1], m.absorb[2]}};
+      uint32_t id = 1;
+      while (id < media.size() && !(media[id].ior == md.ior && media[id].absorb[0] == md.absorb[0] &&
+                                    media[id].absorb[1] == md.absorb[1] && media[id].absorb[2] == md.absorb[2]))
+        id++;
+      if (id == media.size()) {
+        if (media.size() == 32) throw Error{SNOG_EINVAL, "more than 31 distinct glass media (ior, absorb)"};
+        media.push_back(md);
+      }
+      o.medium_id = id;
     }
     if (m.type == SNOG_GLOW && m.underlying >= 0) o.medium_id = mats[m.underlying].medium_id;
   }

@@ -79,7 +79,8 @@ const OctreeArrays &host_octree(SceneImpl &S);
 // the plain render calls use it for the direct integrator.  Synchronous;
 // D_OUT (device) or H_OUT (host) receives the image.
 void render_on_engine(SceneImpl &S, const SnogCamera &cam, const SnogRenderParams &p, float *d_out,
-                      float *h_out, cudaStream_t st, SnogRenderStats *stats);
+                      float *h_out, cudaStream_t st, SnogRenderStats *stats,
+                      const SnogRenderWindow *win = nullptr);
 
 struct Error {
   int code;
@@ -87,6 +88,12 @@ struct Error {
 };
 
 void check_cuda(int err, const char *what);   // throws Error{SNOG_ECUDA}
+
+// Error flags the render kernels raise in their flag word: bit 0, a
+// traversal stack overflowed (a non-finite ray); bit 1, a path entered a
+// fifth nested medium (the path state holds four; the reference's media
+// list is unbounded, material/media.cc:76-118).  Throws for any set flag.
+void check_render_flags(uint32_t flags);
 
 }  // namespace snog
 

@@ -4,8 +4,11 @@
 // random numbers.
 //
 // Everything here follows the reference's formulas and branch structure
-// (files cited per function); it runs in ordinary single precision (FMA
-// allowed) -- images are compared statistically, not bit for bit.
+// (files cited per function), in single precision with every operation
+// rounded on its own: the library is compiled with -fmad=false, so the same
+// shading code inlined into the wave renderer and into the streaming engine
+// gives the same bits and a job's image is the same on either.  Images are
+// compared with the reference's statistically, not bit for bit.
 //
 // Vectors in "normal space" are expressed in the intersection's shading
 // frame, whose z axis is the (possibly flipped) surface normal, as the

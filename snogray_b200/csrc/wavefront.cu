@@ -33,6 +33,7 @@
 
 #include "launch.h"
 #include "pathstate.cuh"
+#include "scene.h"
 #include "wavefront.h"
 
 namespace snog {
@@ -71,13 +72,13 @@ __global__ void __launch_bounds__(256) k_camera(JobConsts jc, uint64_t base, uin
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
     const uint64_t g = base + p;
     const uint32_t pixel = uint32_t(g / jc.S), s = uint32_t(g % jc.S);
-    const int px = int(pixel % jc.PW) - 2, py = int(pixel / jc.PW) - 2;
+    const int px = jc.PX + int(pixel % jc.PW), py = jc.PY + int(pixel / jc.PW);
     Rng rng{jc.seed_lo, jc.seed_hi, uint32_t(g), uint32_t(g >> 32)};
     float2 j = strat_uv(st, rng, pixel, s, dim_of(0, K_CAMERA));
     // Renderer::render_packet (render-mgr/renderer.cc:69-88) and
     // Camera::eye_vec (camera/camera.h:384-389).
     float cu = float(px) + j.x, cv = float(py) + j.y;
-    float fu = cu / float(jc.W), fv = (float(jc.H) - cv) / float(jc.H);
+    float fu = cu / float(jc.FW), fv = (float(jc.FH) - cv) / float(jc.FH);
     float x = 2.f * fu - 1.f, y = 2.f * fv - 1.f;
     float3 d = add(add(load3(jc.cam_fwd), mul(mul(load3(jc.cam_right), x), jc.tan_x)),
                    mul(mul(load3(jc.cam_up), y), jc.tan_y));
@@ -142,7 +143,10 @@ template <int STACK>
 __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_shadow(DevScene s, ShadowQ q, uint32_t *counters, float4 *rad,
                                                       unsigned long long *stats, bool prof) {
   const uint32_t n = counters[2];
-  if (blockIdx.x == 0 && threadIdx.x == 0) stats[1] += n;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    stats[1] += n;
+    stats[6] += counters[6];   // vertices lit this bounce (DirectIllum::sample_all_lights calls)
+  }
   TraceCounters c{0, 0, 0};
   trace_loop<STACK, kAnyOnly>(
       counters + 5, n, c,
@@ -268,9 +272,14 @@ __global__ void __launch_bounds__(128, 6) k_shade(DevScene s, JobConsts jc, uint
           uint32_t nps = (ps & ~0x1ffu) | (len + 1) | ((bs.flags & B_SPECULAR) ? 0x100u : 0u);
           if (bs.flags & B_TRANSMISSIVE) {
             uint32_t mid = s.mats[I.mat].medium_id;
-            if (mid) nps = I.back ? ps_pop(nps) : ps_push(nps, mid);
+            if (mid && I.back) {
+              nps = ps_pop(nps);
+            } else if (mid && !ps_push(nps, mid)) {
+              atomicOr(counters + 3, 2u);   // a fifth nested medium: the path ends here
+              cont = false;
+            }
           }
-          ps = nps;
+          if (cont) ps = nps;
         }
       }
     }
@@ -456,21 +465,24 @@ __global__ void __launch_bounds__(256) k_splat(JobConsts jc, uint64_t base, uint
   // Every lane of a group has the same T, so a group runs its loop together.
   for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G; t < total; t += groups) {
     const int tx = int(t % jc.W), ty = ty0 + int(t / jc.W);
+    // The target pixel on the film; the samples of the pattern pixels within
+    // the filter's reach add to it.
+    const int fx = jc.OX + tx, fy = jc.OY + ty;
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     float wacc = 0.f;
     for (int dy = -2; dy <= 2; dy++) {
-      const int row = ty + dy + 2;
+      const int row = fy + dy - jc.PY;
       if (row < 0 || row >= int(jc.PH)) continue;
       for (int dx = -2; dx <= 2; dx++) {
-        const int col = tx + dx + 2;
+        const int col = fx + dx - jc.PX;
         if (col < 0 || col >= int(jc.PW)) continue;
         const uint32_t pidx = uint32_t(row) * jc.PW + uint32_t(col);
         if (pidx < p0 || pidx >= p1) continue;
         const uint32_t pbase = (pidx - p0) * jc.S;
         for (uint32_t k = sub; k < jc.S; k += G) {
           float2 j = jit[pbase + k];
-          float sx = float(tx + dx) + j.x, sy = float(ty + dy) + j.y;
-          float w = mitchell1(sx - (float(tx) + 0.5f)) * mitchell1(sy - (float(ty) + 0.5f));
+          float sx = float(fx + dx) + j.x, sy = float(fy + dy) + j.y;
+          float w = mitchell1(sx - (float(fx) + 0.5f)) * mitchell1(sy - (float(fy) + 0.5f));
           if (w == 0.f) continue;
           float4 r = rad[pbase + k];
           // Tint (radiance, alpha) stores alpha-scaled colour (color/tint.h:45-49)
@@ -540,21 +552,21 @@ __global__ void __launch_bounds__(256) k_resolve(uint32_t npix, const float4 *ac
 
 template <int STACK>
 void launch_bounce(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, uint64_t base, uint32_t b,
-                   uint32_t cur, uint32_t grid128, cudaStream_t st, RenderProfile *prof) {
+                   uint32_t cur, uint32_t grid128, cudaStream_t st, RenderProfile *prof, bool count) {
   RayQ qin{wb.q_o[cur], wb.q_d[cur], wb.q_path[cur]};
   RayQ qout{wb.q_o[cur ^ 1], wb.q_d[cur ^ 1], wb.q_path[cur ^ 1]};
   ShadowQ sq{wb.s_o, wb.s_d, wb.s_c};
   DirectL dl{wb.d_idx, wb.d_thr};
   PathPtrs P{wb.thr, wb.rad, wb.pstate, wb.jit};
-  const bool pf = prof != nullptr;
-  if (pf) prof->begin(st, RenderProfile::CLOSEST);
+  const bool pf = prof != nullptr || count;
+  if (prof) prof->begin(st, RenderProfile::CLOSEST);
   k_trace_closest<STACK><<<resident_grid(k_trace_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
-  if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADE);
+  if (prof) prof->end(st), prof->begin(st, RenderProfile::SHADE);
   k_shade<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, P, qout, dl);
   k_direct<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, wb.hit_ref, wb.hit_t, dl, sq);
-  if (pf) prof->end(st), prof->begin(st, RenderProfile::SHADOW);
+  if (prof) prof->end(st), prof->begin(st, RenderProfile::SHADOW);
   k_trace_shadow<STACK><<<resident_grid(k_trace_shadow<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(s, sq, wb.counters, wb.rad, wb.stats, pf);
-  if (pf) prof->end(st);
+  if (prof) prof->end(st);
 }
 
 }  // namespace
@@ -661,13 +673,43 @@ void wave_free(WaveBuffers &wb) {
   wb = WaveBuffers{};
 }
 
-JobConsts make_job(const DevScene &s, const SnogCamera &cam, const SnogRenderParams &p) {
+void check_window(const SnogRenderParams &p, const SnogRenderWindow &w) {
+  if (w.pat_width == 0 || w.pat_height == 0 || w.out_width == 0 || w.out_height == 0)
+    throw Error{SNOG_EINVAL, "render window: empty pattern or output"};
+  if (w.out_width > 65536 || w.out_height > 65536 || w.pat_width > 65540 || w.pat_height > 65540)
+    throw Error{SNOG_EINVAL, "render window too large"};
+  const int64_t lim = int64_t(1) << 20;
+  if (w.pat_x < -lim || w.pat_x > lim || w.pat_y < -lim || w.pat_y > lim || w.out_x < -lim || w.out_x > lim ||
+      w.out_y < -lim || w.out_y > lim)
+    throw Error{SNOG_EINVAL, "render window offsets out of range"};
+  if (uint64_t(w.pat_width) * w.pat_height >= (1ull << 32)) throw Error{SNOG_EINVAL, "render pattern too large"};
+  if (uint64_t(w.pat_width) * w.pat_height * p.spp >= (1ull << 40))
+    throw Error{SNOG_EINVAL, "too many paths in one job"};
+}
+
+JobConsts make_job(const DevScene &s, const SnogCamera &cam, const SnogRenderParams &p,
+                   const SnogRenderWindow *win) {
   JobConsts jc;
   std::memset(&jc, 0, sizeof jc);
-  jc.W = p.width;
-  jc.H = p.height;
-  jc.PW = p.width + 4;
-  jc.PH = p.height + 4;
+  jc.FW = p.width;
+  jc.FH = p.height;
+  if (win) {
+    jc.W = win->out_width;
+    jc.H = win->out_height;
+    jc.OX = win->out_x;
+    jc.OY = win->out_y;
+    jc.PW = win->pat_width;
+    jc.PH = win->pat_height;
+    jc.PX = win->pat_x;
+    jc.PY = win->pat_y;
+  } else {
+    jc.W = p.width;
+    jc.H = p.height;
+    jc.OX = jc.OY = 0;
+    jc.PW = p.width + 4;
+    jc.PH = p.height + 4;
+    jc.PX = jc.PY = -2;
+  }
   jc.S = p.spp;
   jc.min_len = p.min_path_len;
   jc.max_len = p.max_path_len;
@@ -699,7 +741,7 @@ JobConsts make_job(const DevScene &s, const SnogCamera &cam, const SnogRenderPar
 
 cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, float4 *accum, float *wsum,
                        float *out_rgb, cudaStream_t st, uint32_t *waves, uint32_t *launches,
-                       RenderProfile *prof) {
+                       RenderProfile *prof, bool count) {
   const uint64_t npix = uint64_t(jc.W) * jc.H;
   cudaError_t e = cudaMemsetAsync(accum, 0, npix * sizeof(float4), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(wsum, 0, npix * sizeof(float), st);
@@ -708,7 +750,7 @@ cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, 
   if (e != cudaSuccess) return e;
   const int sms = num_sms();
   const uint32_t grid128 = uint32_t(sms) * 12, grid256 = uint32_t(sms) * 8;
-  const uint64_t total = uint64_t(jc.PW) * jc.PH * jc.S;
+  const uint64_t total = job_total(jc);
   const uint64_t wave_paths = (wb.wave_cap / jc.S) * jc.S;
   if (wave_paths == 0) return cudaErrorInvalidValue;
   const int sc = stack_class_for_depth(s.max_depth);
@@ -724,18 +766,20 @@ cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, 
     for (uint32_t b = 0; b <= jc.max_len; b++) {
       const uint32_t cur = b & 1u;
       switch (sc) {
-        case 32: launch_bounce<32>(s, jc, wb, base, b, cur, grid128, st, prof); break;
-        case 64: launch_bounce<64>(s, jc, wb, base, b, cur, grid128, st, prof); break;
-        case 128: launch_bounce<128>(s, jc, wb, base, b, cur, grid128, st, prof); break;
-        case 256: launch_bounce<256>(s, jc, wb, base, b, cur, grid128, st, prof); break;
+        case 32: launch_bounce<32>(s, jc, wb, base, b, cur, grid128, st, prof, count); break;
+        case 64: launch_bounce<64>(s, jc, wb, base, b, cur, grid128, st, prof, count); break;
+        case 128: launch_bounce<128>(s, jc, wb, base, b, cur, grid128, st, prof, count); break;
+        case 256: launch_bounce<256>(s, jc, wb, base, b, cur, grid128, st, prof, count); break;
         default: return cudaErrorInvalidValue;
       }
       nl += 4;
     }
-    // Output rows reached by this wave's pattern rows.
+    // Output rows reached by this wave's pattern rows (a sample reaches
+    // the film rows within 2 of its own).
     const uint32_t p0 = uint32_t(base / jc.S), p1 = uint32_t((base + n) / jc.S);
-    int r0 = int(p0 / jc.PW), r1 = int((p1 - 1) / jc.PW);
-    int ty0 = r0 - 4 < 0 ? 0 : r0 - 4, ty1 = r1 > int(jc.H) - 1 ? int(jc.H) - 1 : r1;
+    const int r0 = int(p0 / jc.PW), r1 = int((p1 - 1) / jc.PW);
+    const int a0 = jc.PY + r0 - jc.OY - 2, a1 = jc.PY + r1 - jc.OY + 2;
+    const int ty0 = a0 < 0 ? 0 : a0, ty1 = a1 > int(jc.H) - 1 ? int(jc.H) - 1 : a1;
     if (ty1 >= ty0) {
       if (prof) prof->begin(st, RenderProfile::OTHER);
       launch_splat(jc, base, n, wb.rad, P.jit, accum, wsum, ty0, ty1 - ty0 + 1, grid256, st);

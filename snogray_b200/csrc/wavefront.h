@@ -16,6 +16,9 @@ namespace snog {
 struct JobConsts {
   uint32_t W, H;            // output image
   uint32_t PW, PH;          // render pattern incl. the filter margin
+  int32_t PX, PY;           // film pixel of the pattern's top-left corner (-2, -2 for a whole image)
+  int32_t OX, OY;           // film pixel of the output's top-left corner (0, 0 for a whole image)
+  uint32_t FW, FH;          // film (camera) size, RenderMgr's width x height
   uint32_t S;               // samples per pixel
   uint32_t min_len, max_len, direct_samples;
   float min_trace, bg_alpha, max_trace, horizon;
@@ -55,7 +58,14 @@ uint64_t wave_bytes_per_path(uint32_t n_lights);
 cudaError_t wave_alloc(WaveBuffers &wb, uint64_t cap, uint32_t n_lights);
 void wave_free(WaveBuffers &wb);
 
-JobConsts make_job(const DevScene &s, const SnogCamera &cam, const SnogRenderParams &p);
+// A job's constants.  WIN (may be null: the whole image with the filter
+// margin, as snogray.lua:543-550 builds the pattern) sets the pattern and the
+// output window of a partial render; check_window validates it.
+JobConsts make_job(const DevScene &s, const SnogCamera &cam, const SnogRenderParams &p,
+                   const SnogRenderWindow *win = nullptr);
+void check_window(const SnogRenderParams &p, const SnogRenderWindow &win);
+// Paths a job traces: pattern pixels x samples.
+inline uint64_t job_total(const JobConsts &jc) { return uint64_t(jc.PW) * jc.PH * jc.S; }
 
 // Optional per-kernel timing: CUDA events around every launch of the render,
 // grouped by kernel kind, read back after the render completes.
@@ -75,8 +85,8 @@ struct RenderProfile {
 // Render a whole job on STREAM into accum (float4 colour*weight sums + float
 // weight, W*H each; zeroed here) and resolve it to out_rgb (W*H*3 floats,
 // device).  Paths are processed in waves of at most wb.wave_cap.  With PROF,
-// every launch is bracketed by events and the traversal counts its node
-// visits and primitive tests into wb.stats[2..5].
+// every launch is bracketed by events; with COUNT (or PROF) the traversal
+// counts its node visits and primitive tests into wb.stats[2..5].
 // Mitchell-filter all TOTAL samples of a finished job (radiance + alpha and
 // camera jitter per path, pattern-pixel-major) into its image: clears
 // accum/wsum, gathers, resolves into out_rgb.
@@ -85,7 +95,7 @@ cudaError_t splat_job(const JobConsts &jc, const float4 *rad, const float2 *jit,
 
 cudaError_t render_job(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, float4 *accum,
                        float *wsum, float *out_rgb, cudaStream_t st, uint32_t *waves, uint32_t *launches,
-                       RenderProfile *prof = nullptr);
+                       RenderProfile *prof = nullptr, bool count = false);
 
 }  // namespace snog
 

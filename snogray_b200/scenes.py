@@ -124,6 +124,7 @@ class RenderParams:
     seed: int = 0
     integrator: int = 0                # surface_integ.type: 0 path, 1 direct (direct_samples =
                                        # surface_integ.light_samples)
+    flags: int = 0                     # SNOG_RENDER_* bits (1: count traversal nodes and tests)
 
 
 def material(mtype, color=(0, 0, 0), gloss=(1, 1, 1), m=0.0, ior_n=1.5, ior_k=0.0,
@@ -190,6 +191,122 @@ def direct_params(width=128, height=128, spp=16, seed=0, light_samples=4):
     LIGHT_SAMPLES samples per light."""
     return RenderParams(width=width, height=height, spp=spp, direct_samples=light_samples, integrator=1,
                         seed=seed)
+
+
+# ---------------------------------------------------------------------------
+# The Cornell walls with the remaining materials and lights of the path:
+# Mirror surfaces (the conductor Ior(0.25, 3) that material.mirror uses by
+# default, material/material.lua:232; a dielectric one over a Lambert; one of
+# zero reflectance, which always samples its underlying Lambert,
+# material/mirror.cc:70-80), a glowing sphere (SphereLightSampler,
+# light/sphere-light-sampler.cc:40-194) and an omni point light
+# (light/point-light.cc:78-107).
+
+def _cornell_walls():
+    v = np.array([[0, 0, 0], [1, 0, 0], [1, 0, 1], [0, 0, 1],
+                  [0, 1, 0], [1, 1, 0], [1, 1, 1], [0, 1, 1]], np.float32)
+    tris = np.array([[0, 1, 2], [0, 2, 3], [4, 6, 5], [4, 7, 6], [3, 2, 6], [3, 6, 7],
+                     [0, 3, 7], [0, 7, 4], [1, 5, 6], [1, 6, 2]], np.uint32)
+    tri_mat = np.array([0, 0, 0, 0, 0, 0, 1, 1, 2, 2], np.uint32)
+    return v, tris, tri_mat
+
+
+def mirror_scene():
+    mats = _mats([
+        material(MAT_LAMBERT, (0.73, 0.73, 0.73)),                              # 0 white
+        material(MAT_LAMBERT, (0.65, 0.05, 0.05)),                              # 1 red
+        material(MAT_LAMBERT, (0.12, 0.45, 0.15)),                              # 2 green
+        material(MAT_MIRROR, (0, 0, 0), (0.95, 0.95, 0.95), ior_n=0.25, ior_k=3.0),   # 3 conductor
+        material(MAT_MIRROR, (0.3, 0.3, 0.35), (0.9, 0.9, 0.9), ior_n=1.5),     # 4 dielectric over Lambert
+        material(MAT_MIRROR, (0.5, 0.45, 0.2), (0, 0, 0), ior_n=0.25, ior_k=3.0),   # 5 zero reflectance
+        material(MAT_GLOW, (20.0, 20.0, 20.0)),                                 # 6 sphere light
+    ])
+    v, tris, tri_mat = _cornell_walls()
+    spheres = np.zeros(3, SPHERE_DTYPE)
+    spheres[0] = ((0.3, 0.3, 0.62), 0.3, 3)
+    spheres[1] = ((0.72, 0.2, 0.33), 0.2, 0)
+    spheres[2] = ((0.5, 0.86, 0.45), 0.07, 6)
+    tripars = np.zeros(2, TRIPAR_DTYPE)
+    tripars[0] = ((0.55, 0.3, 0.995), (0.3, 0, 0), (0, 0.45, 0), 1, 4)     # on the back wall
+    tripars[1] = ((0.005, 0.45, 0.15), (0, 0, 0.3), (0, 0.3, 0), 1, 5)     # on the left wall
+    pl = np.zeros(1, PLIGHT_DTYPE)
+    pl[0] = ((0.5, 0.95, 0.2), (0.5, 0.5, 0.45), 2 * math.pi, 0.0, (0, 0, 1))   # omni
+    return SceneData(materials=mats, vertices=v, triangles=tris, tri_mat=tri_mat, spheres=spheres,
+                     tripars=tripars, point_lights=pl, name="mirror")
+
+
+def mirror_params(width=64, height=64, spp=16, seed=0):
+    return RenderParams(width=width, height=height, spp=spp, min_path_len=3, max_path_len=8,
+                        direct_samples=1, seed=seed)
+
+
+# An open scene (y up) lit only by lights that are not surfaces: a spotlight
+# with a fringe (light/point-light.h:42-47, 67-83), a far light of angle 0
+# (an infinitely distant point light, light/far-light.h:35-45) and a far
+# light of non-zero angle (cone sampling, light/far-light.cc:96-156, which
+# also appears as background).  Floor, Cook-Torrance, conductor Mirror and
+# Lambert spheres.
+
+def spot_far_scene():
+    mats = _mats([
+        material(MAT_LAMBERT, (0.6, 0.6, 0.6)),
+        material(MAT_COOK_TORRANCE, (0.6, 0.3, 0.2), (1, 1, 1), m=0.15, ior_n=1.5),
+        material(MAT_MIRROR, (0, 0, 0), (1, 1, 1), ior_n=0.25, ior_k=3.0),
+        material(MAT_LAMBERT, (0.3, 0.5, 0.7)),
+    ])
+    v = np.array([[-1, 0, -1], [2, 0, -1], [2, 0, 2], [-1, 0, 2]], np.float32)
+    tris = np.array([[0, 2, 1], [0, 3, 2]], np.uint32)
+    spheres = np.zeros(3, SPHERE_DTYPE)
+    spheres[0] = ((0.2, 0.25, 0.5), 0.25, 1)
+    spheres[1] = ((0.75, 0.2, 0.45), 0.2, 2)
+    spheres[2] = ((0.5, 0.15, 0.9), 0.15, 3)
+    pl = np.zeros(1, PLIGHT_DTYPE)
+    pl[0] = ((0.5, 1.5, 0.4), (3.0, 3.0, 2.8), math.radians(50.0), math.radians(15.0), (0, -1, 0))
+    fl = np.zeros(2, FLIGHT_DTYPE)
+    d0 = np.array([0.4, 0.8, -0.45])
+    d1 = np.array([-0.5, 0.6, 0.3])
+    fl[0] = (d0 / np.linalg.norm(d0), 0.0, (0.8, 0.75, 0.6))
+    fl[1] = (d1 / np.linalg.norm(d1), math.radians(8.0), (40.0, 42.0, 48.0))
+    return SceneData(materials=mats, vertices=v, triangles=tris, tri_mat=np.zeros(2, np.uint32),
+                     spheres=spheres, point_lights=pl, far_lights=fl, name="spot_far")
+
+
+def spot_far_camera(width, height):
+    cam = Camera()
+    cam.move((0.5, 0.9, -1.3))
+    cam.point((0.5, 0.2, 0.5), (0, 1, 0))
+    cam.set_vert_fov(math.radians(45.0), width / height)
+    return cam
+
+
+# Four concentric Glass spheres of different media in the Cornell box: a
+# path inside the innermost one has four media on its stack
+# (material/media.cc:76-118).
+
+def nested_glass_scene():
+    mats = _mats([
+        material(MAT_LAMBERT, (0.73, 0.73, 0.73)),
+        material(MAT_LAMBERT, (0.65, 0.05, 0.05)),
+        material(MAT_LAMBERT, (0.12, 0.45, 0.15)),
+        material(MAT_GLASS, ior_n=1.3),
+        material(MAT_GLASS, ior_n=1.5, absorb=(0.4, 0.1, 0.05)),
+        material(MAT_GLASS, ior_n=1.7),
+        material(MAT_GLASS, ior_n=1.9, absorb=(0.05, 0.3, 0.6)),
+        material(MAT_GLOW, (15.0, 15.0, 15.0)),
+    ])
+    v, tris, tri_mat = _cornell_walls()
+    spheres = np.zeros(4, SPHERE_DTYPE)
+    for k, r in enumerate((0.32, 0.24, 0.16, 0.08)):
+        spheres[k] = ((0.5, 0.35, 0.5), r, 3 + k)
+    tripars = np.zeros(1, TRIPAR_DTYPE)
+    tripars[0] = ((0.375, 0.999, 0.375), (0, 0, 0.25), (0.25, 0, 0), 1, 7)
+    return SceneData(materials=mats, vertices=v, triangles=tris, tri_mat=tri_mat, spheres=spheres,
+                     tripars=tripars, name="nested_glass")
+
+
+def nested_glass_params(width=64, height=64, spp=16, seed=0):
+    return RenderParams(width=width, height=height, spp=spp, min_path_len=3, max_path_len=14,
+                        direct_samples=1, seed=seed)
 
 
 # ---------------------------------------------------------------------------

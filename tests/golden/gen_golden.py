@@ -148,12 +148,26 @@ RENDER_CASES = {
     "cornell_direct": (scenes.cornell_box, scenes.cornell_camera, scenes.direct_params, 96, 96, 16),
     "mesh_flat_direct": (lambda: scenes.mesh_scene(smooth=False), scenes.mesh_camera, scenes.direct_params,
                          64, 64, 16),
+    # the Cornell workload at its stated size: 256x256, 16 spp, max depth 8
+    "cornell256": (scenes.cornell_box, scenes.cornell_camera, scenes.cornell_params, 256, 256, 16),
+    # Mirror (conductor, dielectric over Lambert, zero reflectance), a sphere
+    # light and an omni point light; both integrators
+    "mirror": (scenes.mirror_scene, scenes.cornell_camera, scenes.mirror_params, 64, 64, 16),
+    "mirror_direct": (scenes.mirror_scene, scenes.cornell_camera, scenes.direct_params, 64, 64, 16),
+    # a spotlight with a fringe and two far lights (angle 0 and 8 degrees)
+    "spot_far": (scenes.spot_far_scene, scenes.spot_far_camera, scenes.mirror_params, 64, 64, 16),
+    "spot_far_direct": (scenes.spot_far_scene, scenes.spot_far_camera, scenes.direct_params, 64, 64, 16),
+    # four nested glass media
+    "nested_glass": (scenes.nested_glass_scene, scenes.cornell_camera, scenes.nested_glass_params,
+                     64, 64, 16),
 }
 
 
 # Renders per side for cases whose median RMSE is too spread at 64 to resolve
-# the 5 % bar (caustics through faceted glass: a bootstrap SD of ~6 % at 64).
-RENDER_K = {"mesh_flat_direct": 1024}
+# the 5 % bar (caustics through faceted or nested glass, small bright lights
+# seen in mirrors: bootstrap SDs of the median of 2-15 % at 64).
+RENDER_K = {"mesh_flat_direct": 1024, "mirror": 256, "mirror_direct": 256, "spot_far": 1024,
+            "spot_far_direct": 2048, "nested_glass": 1024, "cornell256": 1024}
 
 
 def gen_render(name, k=None, gt_spp=4096):
@@ -179,10 +193,41 @@ def gen_render(name, k=None, gt_spp=4096):
           f"gt {info['seconds']:.1f}s")
 
 
+# The terrain workload at its stated size (2,093,058 triangles, 200 spheres,
+# 1024x512 sky, 1920x1080, max depth 16), rendered K times at a low spp;
+# each render is reduced to its per-channel mean and the means of a grid of
+# TILES tiles.
+TERRAIN_FULL = dict(k=32, spp=2, width=1920, height=1080, tiles=(6, 8))
+
+
+def tile_means(img, tiles):
+    ty, tx = tiles
+    h, w, _ = img.shape
+    return img.reshape(ty, h // ty, tx, w // tx, 3).mean((1, 3)).reshape(-1, 3)
+
+
+def gen_terrain_full():
+    c = TERRAIN_FULL
+    sd = scenes.terrain_scene()
+    cam = scenes.terrain_camera(c["width"], c["height"])
+    params = scenes.terrain_params(c["width"], c["height"], c["spp"])
+    red = lambda im: np.concatenate([im.reshape(-1, 3).mean(0)[None], tile_means(im, c["tiles"])])
+    outs, infos = spec.ref_render_repeat(sd, cam, params, c["k"], threads=os.cpu_count() or 8, reduce=red)
+    stats = np.array(outs)                       # (k, 1 + tiles, 3)
+    np.savez_compressed(os.path.join(HERE, "render_terrain_full.npz"), means=stats[:, 0], tiles=stats[:, 1:],
+                        k=c["k"], spp=c["spp"], width=c["width"], height=c["height"],
+                        tile_grid=np.array(c["tiles"]), scene_digest=scenes.scene_digest(sd),
+                        ref_seconds=np.array([i["seconds"] for i in infos]))
+    m = stats[:, 0]
+    print(f"render_terrain_full: mean {m.mean(0)} se {m.std(0, ddof=1) / math.sqrt(len(m))}")
+
+
 if __name__ == "__main__":
     if not spec.have_ref():
         spec.build(["ref"])
-    which = sys.argv[1:] or ["trace", "render"]
+    which = sys.argv[1:] or ["trace", "render", "terrain_full"]
+    if "terrain_full" in which:
+        gen_terrain_full()
     if "trace" in which:
         for nm in TRACE_CASES:
             gen_trace(nm)

@@ -142,3 +142,36 @@ def test_cpp_ply_render_matches_python_render(ply_api, tmp_path):
     assert rec["paths"] == st["paths"]
     assert np.isfinite(img).all() and img.mean() > 0
     assert np.allclose(img, ref, rtol=1e-4, atol=1e-5), np.abs(img - ref).max()
+
+
+# ---- partial renders: RenderPattern, sample-based output, 5-argument render --
+
+LIMIT = dict(w=64, h=48, spp=16, lx=10, ly=8, lw=30, lh=20)
+
+
+@pytest.mark.gpu
+def test_cpp_limit_render_matches_python_window(cornell_api, tmp_path):
+    """The reference driver's --limit set-up through the 5-argument
+    RenderMgr::render gives the same image as the C ABI's window render, and
+    fills the reference's RenderStats fields."""
+    c = LIMIT
+    f32 = str(tmp_path / "img.f32")
+    out = subprocess.run([cornell_api, "limit", str(c["w"]), str(c["h"]), str(c["spp"]), str(c["lx"]), str(c["ly"]),
+                          str(c["lw"]), str(c["lh"]), f32, "5"], check=True, capture_output=True, text=True)
+    rec = json.loads(out.stdout)
+    img = np.fromfile(f32, np.float32).reshape(c["lh"], c["lw"], 3)
+    cam = scenes.cornell_camera(c["w"], c["h"])
+    pattern = (c["lx"] - 2, c["ly"] - 2, c["lw"] + 4, c["lh"] + 4)
+    with sb.Scene(scenes.cornell_box()) as sc:
+        ref, st = sc.render_window(cam, scenes.cornell_params(c["w"], c["h"], c["spp"], seed=5), pattern,
+                                   (c["lx"], c["ly"], c["lw"], c["lh"]))
+    assert rec["paths"] == st["paths"] == (c["lw"] + 4) * (c["lh"] + 4) * c["spp"]
+    assert np.isfinite(img).all() and img.mean() > 0
+    assert np.allclose(img, ref, rtol=1e-4, atol=1e-5), np.abs(img - ref).max()
+    assert rec["scene_intersect_calls"] == rec["closest_rays"] == st["closest_rays"] >= rec["paths"]
+    assert rec["scene_shadow_tests"] == st["shadow_rays"] > 0
+    assert rec["illum_calls"] > 0
+    for k in ("intersect_nodes", "intersect_tests", "shadow_nodes", "shadow_tests"):
+        assert rec[k] > 0, k
+    # every query visits at least the root
+    assert rec["intersect_nodes"] >= rec["scene_intersect_calls"]

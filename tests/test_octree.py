@@ -81,3 +81,23 @@ def test_empty_scene_rejected():
     import snogray_b200 as sb
     with pytest.raises(sb.SnogError):
         Scene(sd, device=False)
+
+
+def test_glass_media_are_shared_and_bounded():
+    """Glass materials with equal ior and absorption share one medium; more
+    than 31 distinct media is refused (the path state's medium ids are 5
+    bits)."""
+    import snogray_b200 as sb
+    base = scenes.random_triangles(8, seed=1)
+    same = scenes._mats([scenes.material(scenes.MAT_GLASS, ior_n=1.5) for _ in range(40)])
+    sph = np.zeros(40, scenes.SPHERE_DTYPE)
+    sph["center"] = np.linspace(0, 1, 40)[:, None]
+    sph["radius"] = 0.01
+    sph["mat"] = np.arange(40)
+    sd = scenes.SceneData(materials=same, vertices=base.vertices, triangles=base.triangles,
+                          tri_mat=np.zeros(8, np.uint32), spheres=sph)
+    sb.Scene(sd, device=False).close()
+    sd.materials = scenes._mats([scenes.material(scenes.MAT_GLASS, ior_n=1.1 + 0.01 * k) for k in range(40)])
+    with pytest.raises(sb.SnogError) as ei:
+        sb.Scene(sd, device=False)
+    assert ei.value.code == sb.SNOG_EINVAL and "31 distinct" in str(ei.value)

@@ -94,3 +94,52 @@ def test_render_stats_and_waves():
     # identical per-path random streams, so identical images up to float
     # summation order in the splat
     assert np.allclose(img1, img2, rtol=1e-5, atol=1e-6)
+
+
+def test_terrain_full_size_means_within_3se(golden):
+    """The terrain workload at its stated size (2,093,058 triangles, 200
+    spheres, 1024x512 sky, 1920x1080, depth 16) against K reference renders
+    at the same low spp: per-channel image means within 3 standard errors,
+    and the means of a 6 x 8 grid of tiles within 4.5 (48 tiles x 3 channels
+    compared at once)."""
+    from gen_golden import TERRAIN_FULL, tile_means
+    g = golden("render_terrain_full.npz")
+    c = TERRAIN_FULL
+    sd = scenes.terrain_scene()
+    assert scenes.scene_digest(sd) == str(g["scene_digest"])
+    cam = scenes.terrain_camera(c["width"], c["height"])
+    k = int(g["k"])
+    means, tiles = [], []
+    with Scene(sd) as sc:
+        for i in range(k):
+            img, _ = sc.render(cam, scenes.terrain_params(c["width"], c["height"], int(g["spp"]), seed=500 + i))
+            assert np.isfinite(img).all() and (img >= 0).all()
+            means.append(img.reshape(-1, 3).mean(0))
+            tiles.append(tile_means(img, c["tiles"]))
+    for ours, ref, bar in ((np.array(means), g["means"], 3.0), (np.array(tiles), g["tiles"], 4.5)):
+        se = np.sqrt(ours.var(0, ddof=1) / len(ours) + ref.var(0, ddof=1) / len(ref))
+        z = np.abs(ours.mean(0) - ref.mean(0)) / np.maximum(se, 1e-12)
+        assert (z < bar).all(), f"max z {z.max():.2f} at {np.unravel_index(z.argmax(), z.shape)}"
+
+
+def test_fifth_nested_medium_is_an_error():
+    """The path state holds four media; a path entering a fifth nested glass
+    ends the render with an error instead of dropping a medium silently
+    (the reference's media list is unbounded, material/media.cc:76-118)."""
+    mats = scenes._mats([scenes.material(scenes.MAT_LAMBERT, (0.5, 0.5, 0.5))] +
+                        [scenes.material(scenes.MAT_GLASS, ior_n=1.2 + 0.1 * k) for k in range(5)] +
+                        [scenes.material(scenes.MAT_GLOW, (5.0, 5.0, 5.0))])
+    sph = np.zeros(6, scenes.SPHERE_DTYPE)
+    for k, r in enumerate((0.4, 0.32, 0.24, 0.16, 0.08)):
+        sph[k] = ((0.5, 0.5, 0.5), r, 1 + k)
+    sph[5] = ((0.5, 0.5, -1.5), 0.3, 6)
+    sd = scenes.SceneData(materials=mats, spheres=sph)
+    cam = scenes.Camera()
+    cam.move((0.5, 0.5, -1.0))
+    cam.point((0.5, 0.5, 0.5), (0, 1, 0))
+    cam.set_vert_fov(math.radians(10.0), 1.0)
+    import snogray_b200 as sb
+    with Scene(sd) as sc:
+        with pytest.raises(sb.SnogError) as ei:
+            sc.render(cam, scenes.RenderParams(16, 16, 4, max_path_len=12))
+    assert ei.value.code == sb.SNOG_EINVAL and "fifth nested medium" in str(ei.value)

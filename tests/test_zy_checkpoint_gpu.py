@@ -122,3 +122,16 @@ def test_checkpoint_errors(cornell, tmp_path):
         with pytest.raises(sb.SnogError) as e:
             srv.submit_resume(slot, bad)
         assert e.value.code == sb.SNOG_EINVAL
+        # a header whose path counts disagree with the job or with the file:
+        # refused before anything is sized from them
+        for total_delta, done_value in ((1, None), (0, 1 << 31)):
+            forged = bytearray(data)
+            total, done = np.frombuffer(bytes(forged[CKP_HEAD:CKP_HEAD + 16]), "<u8")
+            forged[CKP_HEAD:CKP_HEAD + 8] = np.uint64(total + total_delta).tobytes()
+            if done_value is not None:
+                forged[CKP_HEAD + 8:CKP_HEAD + 16] = np.uint64(min(done_value, total)).tobytes()
+            with open(bad, "wb") as f:
+                f.write(bytes(forged))
+            with pytest.raises(sb.SnogError) as e:
+                srv.submit_resume(slot, bad)
+            assert e.value.code == sb.SNOG_EINVAL and "complete snogray_b200 checkpoint" in str(e.value)

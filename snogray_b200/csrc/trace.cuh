@@ -439,21 +439,27 @@ struct Traversal {
     } else {
       // The same tests from shared pieces: per axis the near and far halves'
       // gates, and the child's entry max(t0, lo.x, lo.y, lo.z) and exit
-      // min(t1, hi.x, hi.y, hi.z) built from an x part and a yz part.
-      const bool gx[2] = {t0 < mid.x, t1 > mid.x}, gy[2] = {t0 < mid.y, t1 > mid.y},
-                 gz[2] = {t0 < mid.z, t1 > mid.z};
-      const float in_x[2] = {fmaxf(t0, near_lo.x), fmaxf(t0, mid.x)};
-      const float out_x[2] = {fminf(t1, mid.x), fminf(t1, far.x)};
-      const float in_yz[4] = {fmaxf(near_lo.y, near_lo.z), fmaxf(near_lo.y, mid.z), fmaxf(mid.y, near_lo.z),
-                              fmaxf(mid.y, mid.z)};
-      const float out_yz[4] = {fminf(mid.y, mid.z), fminf(mid.y, far.z), fminf(far.y, mid.z), fminf(far.y, far.z)};
+      // min(t1, hi.x, hi.y, hi.z) built from an x part and a yz part.  The
+      // pieces are scalars picked by selects, not small arrays: an array
+      // indexed in the loop may be placed in local memory, which a node visit
+      // would then write and read a dozen times.
+      const bool gx0 = t0 < mid.x, gx1 = t1 > mid.x, gy0 = t0 < mid.y, gy1 = t1 > mid.y, gz0 = t0 < mid.z,
+                 gz1 = t1 > mid.z;
+      const float in_x0 = fmaxf(t0, near_lo.x), in_x1 = fmaxf(t0, mid.x);
+      const float out_x0 = fminf(t1, mid.x), out_x1 = fminf(t1, far.x);
+      const float in_yz00 = fmaxf(near_lo.y, near_lo.z), in_yz01 = fmaxf(near_lo.y, mid.z),
+                  in_yz10 = fmaxf(mid.y, near_lo.z), in_yz11 = fmaxf(mid.y, mid.z);
+      const float out_yz00 = fminf(mid.y, mid.z), out_yz01 = fminf(mid.y, far.z), out_yz10 = fminf(far.y, mid.z),
+                  out_yz11 = fminf(far.y, far.z);
 #pragma unroll
       for (uint32_t i = 0; i < 8; i++) {
         const uint32_t cb = visit_bits(i);
-        const uint32_t bx = cb >> 2, by = (cb >> 1) & 1u, bz = cb & 1u;
+        const bool bx = (cb & 4u) != 0u, by = (cb & 2u) != 0u, bz = (cb & 1u) != 0u;
         const uint32_t slot = cb ^ oct;
-        const bool ok = ((nd.y >> slot) & 1u) & gx[bx] & gy[by] & gz[bz] &
-                        (fmaxf(in_x[bx], in_yz[2 * by + bz]) < fminf(out_x[bx], out_yz[2 * by + bz]));
+        const float in_yz = by ? (bz ? in_yz11 : in_yz10) : (bz ? in_yz01 : in_yz00);
+        const float out_yz = by ? (bz ? out_yz11 : out_yz10) : (bz ? out_yz01 : out_yz00);
+        const bool ok = ((nd.y >> slot) & 1u) && (bx ? gx1 : gx0) && (by ? gy1 : gy0) && (bz ? gz1 : gz0) &&
+                        (fmaxf(bx ? in_x1 : in_x0, in_yz) < fminf(bx ? out_x1 : out_x0, out_yz));
         vm |= ok ? (1u << i) : 0u;
       }
     }
@@ -589,6 +595,12 @@ __device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool
 #define SNOG_DISPENSE_CHUNK 32
 #endif
 
+// Idle lanes a warp gathers before it refills them (1 = refill at once).
+#ifndef SNOG_REFILL_MIN
+#define SNOG_REFILL_MIN 4
+#endif
+constexpr uint32_t kRefillMin = SNOG_REFILL_MIN;
+
 // Warp-cooperative ray dispenser for the persistent trace kernels: lanes
 // whose ray is finished take the next index from a warp-local range of CHUNK
 // rays, refilled with one atomic on the launch's counter.  All 32 lanes of
@@ -645,8 +657,12 @@ __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, Trac
   bool any = false;
   for (;;) {
     bool all_idle;
-    const uint32_t got =
-        disp.fetch(dispenser, n, ray == RayDispenser::kIdle, ray != RayDispenser::kIdle, &all_idle);
+    // Idle lanes take new rays only once kRefillMin of them are idle: a ray
+    // start (queue loads, root slab set-up, ray slot) then runs on several
+    // lanes at once instead of on one or two every iteration.
+    const uint32_t idle_lanes = __popc(__ballot_sync(0xffffffffu, ray == RayDispenser::kIdle));
+    const bool need = ray == RayDispenser::kIdle && idle_lanes >= kRefillMin;
+    const uint32_t got = disp.fetch(dispenser, n, need, ray != RayDispenser::kIdle, &all_idle);
     if (all_idle) break;
     if (got != RayDispenser::kIdle) {
       ray = got;

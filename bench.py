@@ -20,15 +20,21 @@ the image copied back into pinned host memory every step, wall clock;
 sequence) on the same job.  The path state and queues (several GB) exceed the
 126 MB L2, so no flush is needed between steps.
 
-Two more workloads run after the headline (rank 0, N=1), each against the
-plain renderer doing one job per launch sequence on the same input:
+After the headline (rank 0, N=1): `cornell` -- the Cornell box at 256x256,
+16 spp, depth 8, one job on the plain renderer and on the engine, beside the
+reference on the host cores; `isec` -- 1M random triangles and 16M rays (half
+closest-hit, half any-hit) through snog_trace_device, with its roofline on
+the reference's own traversal counts for a sample of the rays.  Then two
+workloads, each against the plain renderer doing one job per launch sequence
+on the same input:
 `batched` -- 1024 independent random-triangle soups of 1k-50k triangles
 (log-uniform), resolution {64,128,256}^2, spp {4,16,64}, one engine run; and
 `serve` -- 8 resident scenes of 10k-8M triangles, requests at Poisson arrivals
 (random scene, camera, resolution {128..1024}^2, spp {4,16,64}), p50/p95/p99
-latency from arrival to the image in host memory.  The default takes the
-first 200 requests of the stream at 100 requests/s; --serve-requests 2000
---serve-rates 50,200,1000,2000 runs the full sweep.
+latency from arrival to the image in host memory.  The default runs the
+whole stream of 2000 requests at 50 and at 2000 requests/s (the ends of the
+50-2000 sweep; --serve-rates 50,200,1000,2000 adds the middle), reported in
+total and per scene-size class.
 
 Multi-GPU: the path shards trivially (independent paths); each rank renders
 its own job replica (weak scaling), no collective on the data path.  Rank 0
@@ -711,9 +717,9 @@ def main():
     ap.add_argument("--slots", type=int, default=0, help="engine queue slots with --no-autotune")
     ap.add_argument("--batch-jobs", type=int, default=1024,
                     help="jobs of the batched workload (0 = skip it)")
-    ap.add_argument("--serve-requests", type=int, default=200,
-                    help="requests of the serving workload per rate (0 = skip it; 2000 = full stream)")
-    ap.add_argument("--serve-rates", type=str, default="100",
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="requests of the serving workload per rate (0 = skip it)")
+    ap.add_argument("--serve-rates", type=str, default="50,2000",
                     help="comma-separated Poisson arrival rates, requests/s")
     args = ap.parse_args()
     args.serve_rates = [float(x) for x in args.serve_rates.split(",") if x]

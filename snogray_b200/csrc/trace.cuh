@@ -261,7 +261,10 @@ struct Traversal {
   int sp;                    // entries spilled to stk[0, sp)
   bool have;                 // a current entry (node/gate/lo/hi) is set
   const uint4 *nodes;        // the ray's scene (its list and primitive arrays are in the ray slot)
-  StackEntry stk[STACK];
+  // The spilled part of the stack: an array of STACK entries owned by the
+  // caller.  It is not a member: a dynamically indexed member array puts
+  // the whole object in local memory, every scalar above included.
+  StackEntry *stk;
 
   // The ray's origin and direction, from its shared-memory slot.
   __device__ __forceinline__ float3 ray_o() const {
@@ -651,7 +654,9 @@ struct RayDispenser {
 template <int STACK, int ANY = kMixed, class Start, class Done>
 __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, TraceCounters &cnt, Start start,
                                            Done done) {
+  StackEntry stk[STACK];
   Traversal<STACK> tr;
+  tr.stk = stk;
   RayDispenser disp;
   uint32_t ray = RayDispenser::kIdle;
   bool any = false;

@@ -167,10 +167,17 @@ __device__ __forceinline__ bool test_prim(const PrimRec &r, float3 o, float3 d, 
   return false;
 }
 
-// One pending octree visit: node id and gate bits packed into lo.w, the
-// node's parametric slab bounds in lo.xyz (minima) and hi.xyz (maxima).
-struct StackEntry {
-  float4 lo, hi;
+// The pending children of one visited node, as one stack record: the
+// node's near-half lower bounds, midpoints and far-half upper bounds (every
+// child's slab bounds are a selection of these, per axis), its first child's
+// index, its child mask and the visiting positions of the children not yet
+// entered.  One record per visited node with two or more qualifying children,
+// instead of one entry per waiting child: a visit pushes at most once, and
+// the stack holds at most one record per tree level.
+struct StackRec {
+  float4 a;   // near_lo.xyz, first child index
+  float4 b;   // mid.xyz, child mask | visiting positions still to enter << 8
+  float4 c;   // far.xyz
 };
 
 // Threads per block of every trace kernel.
@@ -180,22 +187,21 @@ constexpr int kTraceBlock = 128;
 #define SNOG_TRACE_MINBLOCKS 8
 #endif
 
-// The newest kRing entries of each thread's traversal stack live in shared
-// memory, as a ring; older entries spill to the thread's local-memory array.
-// Lanes of a warp sit at different stack depths, so a local-memory stack is
-// read and written uncoalesced and every push is written through to L2; the
-// ring keeps the pushes and pops of a walk on chip (kRing * 32 bytes per
-// thread, 16 KB per 128-thread block at kRing = 4).
+// The newest kRing records of each thread's stack live in shared memory, as
+// a ring; older ones spill to the thread's local-memory array.  Lanes of a
+// warp sit at different stack depths, so a local-memory stack is read and
+// written uncoalesced; the ring keeps the pushes and pops of a walk on chip
+// (kRing * 48 bytes per thread, 18 KB per 128-thread block at kRing = 3).
 #ifndef SNOG_RING
-#define SNOG_RING 4
+#define SNOG_RING 3
 #endif
 constexpr uint32_t kRing = SNOG_RING;
 
-// This thread's first ring slot.  Entry position e of thread t is float4
-// 2 * e * kTraceBlock + t (lo) and (2 * e + 1) * kTraceBlock + t (hi): a warp
-// touching one position reads 512 contiguous bytes.
+// This thread's first ring slot.  Part k (0, 1, 2) of record position e of
+// thread t is float4 (3 * e + k) * kTraceBlock + t: a warp touching one part
+// of one position reads 512 contiguous bytes.
 __device__ __forceinline__ float4 *ring_slots() {
-  __shared__ float4 ring[2 * kRing * kTraceBlock];
+  __shared__ float4 ring[3 * kRing * kTraceBlock];
   return ring + threadIdx.x;
 }
 
@@ -248,9 +254,10 @@ __device__ __forceinline__ uint32_t visit_bits(uint32_t i) { return i == 3u ? 4u
 // reference's recursive function does: parent gate, slab cull, then the
 // node's surface list (left pending in [lp, lend) for list_round) and the
 // children.  Kernels interleave the steps of many rays per warp and refill
-// lanes whose ray has finished.  STACK + kRing entries must cover
-// 3 * depth + 2 (the host picks STACK from the tree depth); if they do not,
-// cnt.overflow is set and the result must be discarded.
+// lanes whose ray has finished.  The stack holds one record per tree level
+// on the walk's path; kRecs (from STACK, which the host picks from the tree
+// depth) plus kRing records cover every tree the host admits.  Should they
+// not, cnt.overflow is set and the result must be discarded.
 template <int STACK>
 struct Traversal {
   float3 lo, hi;
@@ -261,10 +268,14 @@ struct Traversal {
   int sp;                    // entries spilled to stk[0, sp)
   bool have;                 // a current entry (node/gate/lo/hi) is set
   const uint4 *nodes;        // the ray's scene (its list and primitive arrays are in the ray slot)
-  // The spilled part of the stack: an array of STACK entries owned by the
+  // Records the stack may need: one per tree level.  STACK, the class the
+  // host picks from the tree depth (at least 3 * depth + 4), bounds them
+  // with room to spare.
+  static constexpr int kRecs = (STACK + 2) / 3;
+  // The spilled part of the stack: an array of kRecs records owned by the
   // caller.  It is not a member: a dynamically indexed member array puts
   // the whole object in local memory, every scalar above included.
-  StackEntry *stk;
+  StackRec *stk;
 
   // The ray's origin and direction, from its shared-memory slot.
   __device__ __forceinline__ float3 ray_o() const {
@@ -331,15 +342,17 @@ struct Traversal {
   // The walk is over: no list pending, no current entry, empty stack.
   __device__ __forceinline__ bool finished() const { return lp >= lend && !have && sp == 0 && (ring >> 4) == 0u; }
 
-  // Push an entry: into the ring, first moving the ring's oldest entry to
+  // Push a record: into the ring, first moving the ring's oldest record to
   // local memory when the ring is full.
-  __device__ __forceinline__ void push(float4 elo, float4 ehi, TraceCounters &cnt) {
+  __device__ __forceinline__ void push(float3 nlo, float3 mid, float3 far, uint32_t first, uint32_t bits,
+                                       TraceCounters &cnt) {
     float4 *r = ring_slots();
     uint32_t base = ring & 15u, n = ring >> 4;
     if (n == kRing) {
-      if (sp < STACK) {
-        stk[sp].lo = r[2 * base * kTraceBlock];
-        stk[sp].hi = r[(2 * base + 1) * kTraceBlock];
+      if (sp < kRecs) {
+        stk[sp].a = r[(3 * base) * kTraceBlock];
+        stk[sp].b = r[(3 * base + 1) * kTraceBlock];
+        stk[sp].c = r[(3 * base + 2) * kTraceBlock];
         sp++;
       } else {
         cnt.overflow = 1;
@@ -349,34 +362,47 @@ struct Traversal {
     }
     uint32_t pos = base + n;
     pos = pos >= kRing ? pos - kRing : pos;
-    r[2 * pos * kTraceBlock] = elo;
-    r[(2 * pos + 1) * kTraceBlock] = ehi;
+    r[(3 * pos) * kTraceBlock] = make_float4(nlo.x, nlo.y, nlo.z, __uint_as_float(first));
+    r[(3 * pos + 1) * kTraceBlock] = make_float4(mid.x, mid.y, mid.z, __uint_as_float(bits));
+    r[(3 * pos + 2) * kTraceBlock] = make_float4(far.x, far.y, far.z, 0.f);
     ring = base | ((n + 1u) << 4);
   }
 
-  // Pop the newest entry into the current one.  Returns false (and leaves
-  // the walk unchanged) if nothing is stacked.
+  // Make the next waiting child of the newest record the current entry (the
+  // record is dropped once its last child is taken).  Returns false, leaving
+  // the walk unchanged, if nothing is stacked.
   __device__ __forceinline__ bool pop() {
-    float4 elo, ehi;
-    const uint32_t base = ring & 15u, n = ring >> 4;
-    if (n) {
-      const float4 *r = ring_slots();
-      uint32_t pos = base + n - 1u;
-      pos = pos >= kRing ? pos - kRing : pos;
-      elo = r[2 * pos * kTraceBlock];
-      ehi = r[(2 * pos + 1) * kTraceBlock];
-      ring = n > 1u ? (base | ((n - 1u) << 4)) : 0u;   // an emptied ring restarts at position 0
-    } else if (sp > 0) {
-      --sp;
-      elo = stk[sp].lo;
-      ehi = stk[sp].hi;
-    } else {
-      return false;
+    float4 *r = ring_slots();
+    uint32_t base = ring & 15u, n = ring >> 4;
+    if (n == 0u) {
+      if (sp == 0) return false;
+      --sp;   // bring the newest spilled record back into the ring
+      r[0] = stk[sp].a;
+      r[kTraceBlock] = stk[sp].b;
+      r[2 * kTraceBlock] = stk[sp].c;
+      base = 0u;
+      n = 1u;
     }
-    node = __float_as_uint(elo.w);
-    gate = __float_as_uint(ehi.w);
-    lo = xyz(elo);
-    hi = xyz(ehi);
+    uint32_t pos = base + n - 1u;
+    pos = pos >= kRing ? pos - kRing : pos;
+    const float4 ra = r[(3 * pos) * kTraceBlock], rb = r[(3 * pos + 1) * kTraceBlock],
+                 rc = r[(3 * pos + 2) * kTraceBlock];
+    const uint32_t bits = __float_as_uint(rb.w);
+    const uint32_t vm = bits >> 8;
+    const uint32_t i = __ffs(vm) - 1u;   // the earliest visiting position left
+    const uint32_t rest = vm & (vm - 1u);
+    if (rest) {
+      reinterpret_cast<uint32_t *>(r + (3 * pos + 1) * kTraceBlock)[3] = (bits & 0xffu) | (rest << 8);
+      ring = base | (n << 4);
+    } else {
+      ring = n > 1u ? (base | ((n - 1u) << 4)) : 0u;   // an emptied ring restarts at position 0
+    }
+    const uint32_t cb = visit_bits(i);
+    const uint32_t slot = cb ^ (octant & 7u);
+    node = __float_as_uint(ra.w) + __popc(bits & 0xffu & ((1u << slot) - 1u));
+    gate = cb | kGateFlag;
+    lo = f3((cb & 4) ? rb.x : ra.x, (cb & 2) ? rb.y : ra.y, (cb & 1) ? rb.z : ra.z);
+    hi = f3((cb & 4) ? rc.x : rb.x, (cb & 2) ? rc.y : rb.y, (cb & 1) ? rc.z : rb.z);
     return true;
   }
 
@@ -467,21 +493,11 @@ struct Traversal {
       }
     }
     if (!vm) return;
-    // Every qualifying child but the first is pushed, in reverse visiting
-    // order, so they pop in visiting order after the first child's subtree;
-    // the first becomes the current entry.
-    for (uint32_t m = vm & (vm - 1u); m;) {
-      const uint32_t i = 31u - __clz(m);
-      m &= ~(1u << i);
-      const uint32_t cb = visit_bits(i);
-      const uint32_t slot = cb ^ oct;
-      const uint32_t c = nd.x + __popc(nd.y & ((1u << slot) - 1u));
-      push(make_float4((cb & 4) ? mid.x : near_lo.x, (cb & 2) ? mid.y : near_lo.y, (cb & 1) ? mid.z : near_lo.z,
-                       __uint_as_float(c)),
-           make_float4((cb & 4) ? far.x : mid.x, (cb & 2) ? far.y : mid.y, (cb & 1) ? far.z : mid.z,
-                       __uint_as_float(cb | kGateFlag)),
-           cnt);
-    }
+    // The first qualifying child becomes the current entry; the others wait
+    // in one record and are entered in visiting order after the first
+    // child's subtree (pop), as the reference's loop over the children does.
+    const uint32_t rest = vm & (vm - 1u);
+    if (rest) push(near_lo, mid, far, nd.x, (nd.y & 0xffu) | (rest << 8), cnt);
     const uint32_t i = __ffs(vm) - 1u;
     const uint32_t cb = visit_bits(i);
     const uint32_t slot = cb ^ oct;
@@ -654,7 +670,7 @@ struct RayDispenser {
 template <int STACK, int ANY = kMixed, class Start, class Done>
 __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, TraceCounters &cnt, Start start,
                                            Done done) {
-  StackEntry stk[STACK];
+  StackRec stk[Traversal<STACK>::kRecs];
   Traversal<STACK> tr;
   tr.stk = stk;
   RayDispenser disp;

@@ -31,6 +31,10 @@ uint32_t resident_grid(K kernel, int threads) {
   return uint32_t(per_sm) * uint32_t(num_sms());
 }
 
+// Fill lrec (3 float4 per slot) from the surface lists and primitive records.
+cudaError_t build_list_records(const uint32_t *plist, uint32_t n, const float4 *prims, float4 *lrec,
+                               cudaStream_t st);
+
 // Stack class (entries) for an octree of the given depth, 0 if too deep.
 int stack_class_for_depth(uint32_t depth);
 

@@ -5,6 +5,7 @@
 // Compiled with -ffp-contract=off: bounding boxes, edges and midpoints must
 // round exactly as the reference's float code does.
 
+#include "launch.h"
 #include "scene.h"
 
 #include "octree_gpu.h"
@@ -486,8 +487,15 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
       std::vector<uint4> nodes = compact_nodes(S.oct, plist4);
       D.nodes = dev_upload(A, nodes);
       D.plist = dev_upload(A, plist4);
+      S.oct_plist4 = uint32_t(plist4.size());
     }
     D.prims = dev_upload(A, prims);
+    {
+      float4 *lrec = static_cast<float4 *>(A.alloc(size_t(S.oct_plist4) * 48));
+      check_cuda(build_list_records(D.plist, S.oct_plist4, D.prims, lrec, nullptr), "list records");
+      check_cuda(cudaStreamSynchronize(nullptr), "list records");
+      D.lrec = lrec;
+    }
     D.prim_mat = dev_upload(A, prim_mat);
     if (d.vertex_normals && d.n_triangles) {
       std::vector<float4> vn(d.n_vertices);

@@ -7,8 +7,12 @@
 //                                         list start, list length (below)
 //   plist          uint32[n_plist]        surface lists of primitive ids; each
 //                                         list starts at a multiple of 4 and
-//                                         is padded with PREF_END to one, so
-//                                         4 ids come with one 128-bit load
+//                                         is padded with PREF_END to one
+//   lrec           float4[3 * n_plist]    the surface lists again, as the
+//                                         primitives' 48-byte records in list
+//                                         order with the id in c.w: a list
+//                                         test reads one record, not an id
+//                                         and then a record
 //   prims          float4[3 * n_prims]    one 48-byte record per primitive,
 //                                         indexed by primitive id (triangles,
 //                                         then spheres, then tripars):
@@ -91,6 +95,7 @@ struct DevMedium {
 struct DevScene {
   const uint4 *nodes;
   const uint32_t *plist;
+  const float4 *lrec;         // 3 per plist slot: the primitive record of the slot's id, id in c.w
   const float4 *prims;
   const uint32_t *prim_mat;
   const DevMaterial *mats;

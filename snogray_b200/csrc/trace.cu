@@ -90,6 +90,34 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_BATCH_MINBLOCKS) k_tra
 
 // Stack depth needed for a tree of depth D: at most 3 pending entries per
 // level (4 children can pass, one is entered), plus slack.
+// One 48-byte primitive record per surface-list slot, in list order: the
+// record of the slot's primitive id, with the id in c.w (padding slots get a
+// zero record, never read).
+__global__ void k_list_records(const uint32_t *__restrict__ plist, uint32_t n, const float4 *__restrict__ prims,
+                               float4 *__restrict__ lrec) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t id = plist[i];
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a;
+    if (id != PREF_END) {
+      a = prims[3 * size_t(id)];
+      b = prims[3 * size_t(id) + 1];
+      c = prims[3 * size_t(id) + 2];
+      c.w = __uint_as_float(id);
+    }
+    lrec[3 * size_t(i)] = a;
+    lrec[3 * size_t(i) + 1] = b;
+    lrec[3 * size_t(i) + 2] = c;
+  }
+}
+
+cudaError_t build_list_records(const uint32_t *plist, uint32_t n, const float4 *prims, float4 *lrec,
+                               cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const uint32_t blocks = (n + 255) / 256 < 65535u ? (n + 255) / 256 : 65535u;
+  k_list_records<<<blocks, 256, 0, st>>>(plist, n, prims, lrec);
+  return cudaGetLastError();
+}
+
 int stack_class_for_depth(uint32_t depth) {
   uint32_t need = 3 * depth + 4;
   if (need <= 32) return 32;

@@ -208,7 +208,7 @@ __device__ __forceinline__ float4 *ring_slots() {
 // Each thread's current ray in shared memory, for the lanes that test its
 // list entries (a list round would otherwise move 14 values by shuffles):
 // uint4 k * kTraceBlock + threadIdx.x holds, for k = 0, 1, 2, (origin, t0),
-// (direction, t1) and the scene's list and primitive pointers.
+// (direction, t1) and the scene's list-record pointer.
 __device__ __forceinline__ uint4 *ray_slots() {
   __shared__ uint4 rays[3 * kTraceBlock];
   return rays;
@@ -305,11 +305,11 @@ struct Traversal {
     nodes = s.nodes;
     {
       uint4 *slot = ray_slots() + threadIdx.x;
-      const unsigned long long pl = reinterpret_cast<uintptr_t>(s.plist), pr = reinterpret_cast<uintptr_t>(s.prims);
+      const unsigned long long pl = reinterpret_cast<uintptr_t>(s.lrec);
       slot[0] = make_uint4(__float_as_uint(o.x), __float_as_uint(o.y), __float_as_uint(o.z), __float_as_uint(t0_));
       slot[kTraceBlock] =
           make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z), __float_as_uint(t1_));
-      slot[2 * kTraceBlock] = make_uint4(uint32_t(pl), uint32_t(pl >> 32), uint32_t(pr), uint32_t(pr >> 32));
+      slot[2 * kTraceBlock] = make_uint4(uint32_t(pl), uint32_t(pl >> 32), 0u, 0u);
     }
     // 1 / d rounded once, as the reference's division (__frcp_rn is the
     // correctly rounded reciprocal, the same value as 1.0f / d).
@@ -574,11 +574,11 @@ __device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool
     const float rt0 = __uint_as_float(ra.w);
     th = __uint_as_float(rb.w);
     const uint4 rc = slot[2 * kTraceBlock];
-    const unsigned long long o_plist = (unsigned long long)rc.x | ((unsigned long long)rc.y << 32);
-    const unsigned long long o_prims = (unsigned long long)rc.z | ((unsigned long long)rc.w << 32);
-    pid = __ldg(reinterpret_cast<const uint32_t *>(o_plist) + o_lp + (lane - o_excl));
-    const float4 *p = reinterpret_cast<const float4 *>(o_prims) + 3 * size_t(pid);
+    // The entry's primitive record from the owner's scene's list records.
+    const unsigned long long o_lrec = (unsigned long long)rc.x | ((unsigned long long)rc.y << 32);
+    const float4 *p = reinterpret_cast<const float4 *>(o_lrec) + 3 * size_t(o_lp + (lane - o_excl));
     const PrimRec r{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+    pid = __float_as_uint(r.c.w);
     hit = test_prim(r, ro, rd, rt0, th);
   }
   // Reduce over each owner's entries (positive t: its bits order like the value).

@@ -620,6 +620,12 @@ __device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool
 #endif
 constexpr uint32_t kRefillMin = SNOG_REFILL_MIN;
 
+// Pending list entries a closest-hit warp gathers before a list round.
+#ifndef SNOG_ROUND_MIN
+#define SNOG_ROUND_MIN 24
+#endif
+constexpr uint32_t kRoundMin = SNOG_ROUND_MIN;
+
 // Warp-cooperative ray dispenser for the persistent trace kernels: lanes
 // whose ray is finished take the next index from a warp-local range of CHUNK
 // rays, refilled with one atomic on the launch's counter.  All 32 lanes of
@@ -696,7 +702,19 @@ __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, Trac
     const uint32_t pend = (busy && tr.lp < tr.lend) ? tr.lend - tr.lp : 0u;
     const uint32_t pending = __reduce_add_sync(0xffffffffu, pend < 32u ? pend : 32u);
     if (pending < 32u && busy && tr.lp >= tr.lend && !tr.finished()) tr.template node_step<true, ANY>(cnt);
-    const bool stop = list_round(tr, busy && tr.lp < tr.lend, any, cnt);
+    // Closest-hit kernels test lists only once at least kRoundMin entries
+    // are pending, unless no lane could visit a node: fewer, fuller rounds
+    // (2 % off the terrain frame; the any-hit and mixed kernels, whose
+    // lists are longer or whose walks end early, measured no gain or a
+    // loss).
+    bool round = true;
+    if (ANY == kClosestOnly) {
+      const uint32_t pend2 = (busy && tr.lp < tr.lend) ? tr.lend - tr.lp : 0u;
+      const uint32_t pending2 = __reduce_add_sync(0xffffffffu, pend2 < 32u ? pend2 : 32u);
+      const bool can_step = busy && tr.lp >= tr.lend && !tr.finished();
+      round = pending2 >= kRoundMin || __ballot_sync(0xffffffffu, can_step) == 0u;
+    }
+    const bool stop = round && list_round(tr, busy && tr.lp < tr.lend, any, cnt);
     if (busy && (stop || tr.finished())) {
       done(ray, tr, any);
       ray = RayDispenser::kIdle;

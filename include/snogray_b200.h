@@ -173,6 +173,11 @@ typedef struct SnogSceneInfo {
   float horizon;
   uint64_t device_bytes;
   double build_ms;
+  /* 1 when the closest-hit traversal deals list entries to lanes in pairs
+   * for this scene: random rays through it test more than 2.5 primitives per
+   * node visit (long lists along rays); decided when the scene is created. */
+  uint32_t pair_lists;
+  uint32_t reserved;
 } SnogSceneInfo;
 
 typedef struct SnogRenderStats {

@@ -91,7 +91,8 @@ class SnogSceneInfo(C.Structure):
                 ("n_spheres", C.c_uint32), ("n_tripars", C.c_uint32), ("n_lights", C.c_uint32),
                 ("n_list_surfaces", C.c_uint64), ("origin", C.c_float * 3), ("size", C.c_float),
                 ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("horizon", C.c_float),
-                ("device_bytes", C.c_uint64), ("build_ms", C.c_double)]
+                ("device_bytes", C.c_uint64), ("build_ms", C.c_double), ("pair_lists", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class SnogRenderStats(C.Structure):

@@ -127,14 +127,14 @@ __global__ void __launch_bounds__(256) k_e_regen(EngineCtl *ctl, const WorkItem 
   }
 }
 
-template <int STACK>
+template <int STACK, int PER>
 __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_e_closest(EngineCtl *ctl, uint32_t cur, const EngineJobDev *jobs,
                                                       const DevScene *scenes, EQ q, uint32_t *hit_ref,
                                                       float *hit_t) {
   const uint32_t n = ctl->qcount[cur];
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl->rays_closest += n;
   TraceCounters c{0, 0, 0};
-  trace_loop<STACK, kClosestOnly>(
+  trace_loop<STACK, kClosestOnly, PER>(
       &ctl->disp_closest, n, c,
       [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
         const float4 o = q.o[ray], d = q.d[ray];
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(128, SNOG_DIRECT_MINBLOCKS) k_e_direct(EngineC
 // One iteration's kernel sequence on ST.  EV (null while capturing a graph)
 // receives five events: before plan, before closest, before shade (shading and
 // direct lighting), before shadow, after shadow.
-template <int STACK>
+template <int STACK, int PER>
 void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uint32_t R, uint32_t N,
                       uint32_t cur, const EngineJobDev *jobs, const DevScene *scenes, EQ qc, EQ qn,
                       uint32_t *hit_ref, float *hit_t, EDL dl, ESQ sq, unsigned long long *job_done,
@@ -560,8 +560,8 @@ void launch_iteration(cudaStream_t st, EngineCtl *ctl, const WorkItem *ring, uin
   k_e_plan<<<1, 1, 0, st>>>(ctl, ring, R, N, cur, sp_cap);
   k_e_regen<<<sms * 8, 256, 0, st>>>(ctl, ring, R, jobs, qc, sp, sp_cap);
   if (ev) cudaEventRecord(ev[1], st);
-  k_e_closest<STACK><<<resident_grid(k_e_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref,
-                                                                               hit_t);
+  k_e_closest<STACK, PER><<<resident_grid(k_e_closest<STACK, PER>, kTraceBlock), kTraceBlock, 0, st>>>(
+      ctl, cur, jobs, scenes, qc, hit_ref, hit_t);
   if (ev) cudaEventRecord(ev[2], st);
   if (direct) {
     k_e_shade<true><<<sms * 12, 128, 0, st>>>(ctl, cur, jobs, scenes, qc, hit_ref, hit_t, qn, dl, job_done,
@@ -699,8 +699,9 @@ Engine::Engine(const EngineConfigHost &cfg, cudaStream_t stream) : cfg_(cfg) {
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto &kv : jobs_) release_job(kv.second);
-  for (cudaGraphExec_t &gx : graph_)
-    if (gx) cudaGraphExecDestroy(gx);
+  for (auto &row : graph_)
+    for (cudaGraphExec_t &gx : row)
+      if (gx) cudaGraphExecDestroy(gx);
   cache_.trim();
   cudaFree(block_);
   cudaFreeHost(ctl_host_);
@@ -740,10 +741,11 @@ uint32_t Engine::add_scene(SceneImpl *scene) {
   check_cuda(cudaStreamSynchronize(stream_), "scene table");
   const int sc = stack_class_for_depth(scene->dev.max_depth);
   if (sc > graph_stack_) {
-    for (cudaGraphExec_t &gx : graph_) {
-      if (gx) cudaGraphExecDestroy(gx);
-      gx = nullptr;
-    }
+    for (auto &row : graph_)
+      for (cudaGraphExec_t &gx : row) {
+        if (gx) cudaGraphExecDestroy(gx);
+        gx = nullptr;
+      }
     graph_stack_ = sc;
   }
   return slot;
@@ -751,7 +753,7 @@ uint32_t Engine::add_scene(SceneImpl *scene) {
 
 // Every iteration of one launch (iters_per_launch pairs, queue 0 -> 1 -> 0),
 // with events around the kernels while profiling.
-void Engine::launch_iterations(bool direct) {
+void Engine::launch_iterations(bool direct, bool pair) {
   EQ q[2];
   for (int k = 0; k < 2; k++) q[k] = EQ{q_o_[k], q_d_[k], q_thr_[k], q_rad_[k], q_meta_[k]};
   ESQ sq{s_o_, s_d_, s_c_, s_tgt_};
@@ -766,30 +768,35 @@ void Engine::launch_iterations(bool direct) {
   for (uint32_t it = 0; it < n_iter; it++) {
     const uint32_t cur = it & 1u;
     const cudaEvent_t *ev = profile_on_ ? &events_[5 * it] : nullptr;
-#define SNOG_ITER(S)                                                                                          \
-  launch_iteration<S>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], \
-                      q[cur ^ 1], hit_ref_, hit_t_, EDL{d_idx_, d_tgt_}, sq, job_done_, job_done_ + cfg_.max_jobs,            \
-                      EQ{sp_o_, sp_d_, sp_thr_, sp_rad_, sp_meta_}, sp_cap_, direct, ev)
-    switch (graph_stack_) {
-      case 32: SNOG_ITER(32); break;
-      case 64: SNOG_ITER(64); break;
-      case 128: SNOG_ITER(128); break;
-      default: SNOG_ITER(256); break;
+#define SNOG_ITER(S, P)                                                                                     \
+  launch_iteration<S, P>(stream_, ctl_, ring_, cfg_.ring_items, cfg_.slots, cur, jobs_dev_, scenes_dev_, q[cur], \
+                         q[cur ^ 1], hit_ref_, hit_t_, EDL{d_idx_, d_tgt_}, sq, job_done_,                      \
+                         job_done_ + cfg_.max_jobs, EQ{sp_o_, sp_d_, sp_thr_, sp_rad_, sp_meta_}, sp_cap_,     \
+                         direct, ev)
+    switch (graph_stack_ * 2 + (pair ? 1 : 0)) {
+      case 64: SNOG_ITER(32, 1); break;
+      case 65: SNOG_ITER(32, 2); break;
+      case 128: SNOG_ITER(64, 1); break;
+      case 129: SNOG_ITER(64, 2); break;
+      case 256: SNOG_ITER(128, 1); break;
+      case 257: SNOG_ITER(128, 2); break;
+      case 513: SNOG_ITER(256, 2); break;
+      default: SNOG_ITER(256, 1); break;
     }
 #undef SNOG_ITER
   }
 }
 
-void Engine::build_graph(bool direct) {
+void Engine::build_graph(bool direct, bool pair) {
   cudaGraph_t g;
   const bool prof = profile_on_;
   profile_on_ = false;
   check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
-  launch_iterations(direct);
+  launch_iterations(direct, pair);
   profile_on_ = prof;
   cudaError_t e = cudaStreamEndCapture(stream_, &g);
   check_cuda(e, "end capture");
-  e = cudaGraphInstantiate(&graph_[direct], g, 0);
+  e = cudaGraphInstantiate(&graph_[direct][pair], g, 0);
   cudaGraphDestroy(g);
   check_cuda(e, "graph instantiate");
 }
@@ -1087,12 +1094,21 @@ bool Engine::step() {
   bool direct = false;
   for (size_t k = 0; k < active_.size() && !direct; k++)
     direct = jobs_.at(active_[k]).jc.integ == SNOG_INTEG_DIRECT;
+  // Closest-hit rounds deal list entries in pairs while most of the active
+  // jobs' remaining paths are in scenes with long lists along rays.
+  uint64_t paired = 0, single = 0;
+  for (size_t k = 0; k < active_.size(); k++) {
+    const HostJob &j = jobs_.at(active_[k]);
+    const uint64_t left = j.total > rays_done(j) ? j.total - rays_done(j) : 0;
+    (scenes_[j.scene_slot]->dev.pair_lists ? paired : single) += left;
+  }
+  const bool pair = paired > single;
   if (work) {
     if (profile_on_) {
-      launch_iterations(direct);
+      launch_iterations(direct, pair);
     } else {
-      if (!graph_[direct]) build_graph(direct);
-      check_cuda(cudaGraphLaunch(graph_[direct], stream_), "graph launch");
+      if (!graph_[direct][pair]) build_graph(direct, pair);
+      check_cuda(cudaGraphLaunch(graph_[direct][pair], stream_), "graph launch");
     }
     kernel_launches_ += 6 * 2 * cfg_.iters_per_launch;
     check_cuda(cudaMemcpyAsync(ctl_host_, ctl_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_), "ctl");

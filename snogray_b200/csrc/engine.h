@@ -204,8 +204,8 @@ class Engine {
   // when every path and every spawned ray has finished).
   uint64_t rays_done(const HostJob &j) const { return done_host_[j.table_slot]; }
   uint64_t rays_spawned(const HostJob &j) const { return done_host_[cfg_.max_jobs + j.table_slot]; }
-  void build_graph(bool direct);
-  void launch_iterations(bool direct);
+  void build_graph(bool direct, bool pair);
+  void launch_iterations(bool direct, bool pair);
   void admit();
   void push_items();
   void release_job(HostJob &j);
@@ -217,7 +217,8 @@ class Engine {
   bool profile_on_ = false;
   Profile prof_;
   std::vector<cudaEvent_t> events_;
-  cudaGraphExec_t graph_[2] = {nullptr, nullptr};   // [with the direct integrator's shading]
+  // [with the direct integrator's shading][closest-hit rounds in pairs]
+  cudaGraphExec_t graph_[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int graph_stack_ = 0;
   // device buffers
   void *block_ = nullptr;

@@ -35,6 +35,12 @@ uint32_t resident_grid(K kernel, int threads) {
 cudaError_t build_list_records(const uint32_t *plist, uint32_t n, const float4 *prims, float4 *lrec,
                                cudaStream_t st);
 
+// Whether the closest-hit kernels should deal list entries in pairs for
+// scene S: traces 8192 random rays through its bounding box and answers yes
+// when they test more than 2.5 primitives per node visit (long lists along
+// rays, as in random-triangle soups: 4.8; the terrain: 1.2).
+uint32_t probe_pair_lists(const DevScene &s);
+
 // Stack class (entries) for an octree of the given depth, 0 if too deep.
 int stack_class_for_depth(uint32_t depth);
 

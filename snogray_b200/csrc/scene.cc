@@ -544,6 +544,7 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
   D.horizon = horizon;
   D.max_depth = S.oct.max_depth;
   D.right_handed = d.mesh_right_handed ? 1u : 0u;
+  D.pair_lists = upload ? probe_pair_lists(D) : 0u;
 
   SnogSceneInfo &I = S.info;
   std::memset(&I, 0, sizeof(I));
@@ -565,6 +566,7 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
   I.horizon = horizon;
   I.device_bytes = A.bytes;
   I.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  I.pair_lists = D.pair_lists;
   return sc.release();
 }
 

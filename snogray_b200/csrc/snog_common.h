@@ -113,6 +113,7 @@ struct DevScene {
   float mesh_center[3];       // midpoint of the mesh bounding box (mesh.cc:581)
   float horizon;              // scene bbox diameter (render/scene.cc:28)
   uint32_t max_depth;         // octree depth, sizes the traversal stack
+  uint32_t pair_lists;        // closest-hit rounds deal list entries in pairs (long lists along rays)
   uint32_t right_handed;      // mesh geometric normal e1 x e2 (else e2 x e1)
   const float4 *vnormals;     // per vertex, or null: no interpolated normals
   const uint4 *tri_vidx;      // per triangle, its vertex indices (with vnormals)

@@ -6,7 +6,11 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <vector>
+
 #include "launch.h"
+#include "scene.h"
 #include "trace.cuh"
 
 namespace snog {
@@ -116,6 +120,46 @@ cudaError_t build_list_records(const uint32_t *plist, uint32_t n, const float4 *
   const uint32_t blocks = (n + 255) / 256 < 65535u ? (n + 255) / 256 : 65535u;
   k_list_records<<<blocks, 256, 0, st>>>(plist, n, prims, lrec);
   return cudaGetLastError();
+}
+
+uint32_t probe_pair_lists(const DevScene &s) {
+  constexpr uint32_t n = 8192;
+  if (!s.n_nodes || !stack_class_for_depth(s.max_depth)) return 0;
+  // Random rays through the scene's bounding box (fixed seed: the choice is
+  // the same every time the scene is built).
+  std::vector<float> rays(size_t(n) * 7);
+  uint64_t x = 0x9e3779b97f4a7c15ull;
+  auto uni = [&x]() {
+    x ^= x << 13;
+    x ^= x >> 7;
+    x ^= x << 17;
+    return float(double(x >> 40) * (1.0 / 16777216.0));
+  };
+  for (uint32_t i = 0; i < n; i++) {
+    for (int k = 0; k < 3; k++) rays[size_t(k) * n + i] = s.bbox_min[k] + (s.bbox_max[k] - s.bbox_min[k]) * uni();
+    const float z = 2.f * uni() - 1.f, phi = 6.2831853f * uni(), r = std::sqrt(std::fmax(0.f, 1.f - z * z));
+    rays[3 * size_t(n) + i] = r * std::cos(phi);
+    rays[4 * size_t(n) + i] = r * std::sin(phi);
+    rays[5 * size_t(n) + i] = z;
+    rays[6 * size_t(n) + i] = INFINITY;
+  }
+  char *block = nullptr;
+  const size_t rb = rays.size() * 4, pb = size_t(n) * 4;
+  check_cuda(cudaMalloc(&block, rb + pb + 64), "probe buffers");
+  unsigned long long cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  cudaError_t e = cudaMemcpy(block, rays.data(), rb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(block + rb + pb, 0, 64);
+  if (e == cudaSuccess) {
+    unsigned long long *c = reinterpret_cast<unsigned long long *>(block + rb + pb);
+    e = launch_trace_batch(s, reinterpret_cast<const float *>(block), n, n, reinterpret_cast<int32_t *>(block + rb),
+                           nullptr, nullptr, c, reinterpret_cast<uint32_t *>(c) + 8, reinterpret_cast<uint32_t *>(c) + 9,
+                           nullptr, nullptr);
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(cnt, block + rb + pb, 64, cudaMemcpyDeviceToHost);
+  cudaFree(block);
+  check_cuda(e, "list probe");
+  // cnt[0]: node visits, cnt[1]: primitive tests of the closest-hit queries
+  return cnt[1] > 5 * cnt[0] / 2 ? 1u : 0u;
 }
 
 int stack_class_for_depth(uint32_t depth) {

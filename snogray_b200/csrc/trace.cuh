@@ -561,15 +561,17 @@ __device__ __forceinline__ uint32_t nth_set_bit(uint32_t mask, uint32_t k) {
 // Test counts are the reference's (all entries, or up to the stopping one).
 // All 32 lanes must call it together.  Returns true for an any-hit lane whose
 // search is over.
-template <int STACK, int ANY = kMixed>
+// PER: entries dealt to a lane per round, 1 or 2.  Pairs (two consecutive
+// entries of one list per lane, up to 64 per round) pay where the lists a
+// ray meets are long: the ray-batch kernel uses them (random-triangle
+// batches: 11 % faster), and the closest-hit kernels do for scenes whose
+// probe found long lists along rays (SceneImpl's pair_lists: 8 % faster on
+// a 2M-triangle soup, 3 % slower on the terrain, whose lists are short).
+// Any-hit rounds deal single entries: a walk stops at its first hit.
+template <int STACK, int ANY = kMixed, int PER = (ANY == kMixed ? 2 : 1)>
 __device__ __forceinline__ bool list_round(Traversal<STACK> &tr, bool want, bool any, TraceCounters &cnt) {
   constexpr unsigned kFull = 0xffffffffu;
-  // The mixed kernel (ray batches) deals entries in pairs: a lane tests two
-  // consecutive entries of one list, a round up to 64 -- on the long lists
-  // of random-triangle batches that measured 11 % faster.  The renderer's
-  // kernels deal single entries: their lists are short (pairs measured 7 %
-  // slower on the terrain frame), and an any-hit walk stops at its first hit.
-  constexpr uint32_t kPer = ANY == kMixed ? 2u : 1u;
+  constexpr uint32_t kPer = uint32_t(PER);
   const uint32_t lane = threadIdx.x & 31u;
   __syncwarp();   // the warp's ray-slot writes (new rays, shrunk t1) are visible
   uint32_t c = want ? tr.lend - tr.lp : 0u;
@@ -721,7 +723,7 @@ struct RayDispenser {
 // round of list entries pending, every live lane without a list pending
 // visits one octree entry; then the warp tests one round of pending list
 // entries together.  All 32 lanes of every warp must run it.
-template <int STACK, int ANY = kMixed, class Start, class Done>
+template <int STACK, int ANY = kMixed, int PER = (ANY == kMixed ? 2 : 1), class Start, class Done>
 __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, TraceCounters &cnt, Start start,
                                            Done done) {
   StackRec stk[Traversal<STACK>::kRecs];
@@ -762,7 +764,7 @@ __device__ __forceinline__ void trace_loop(uint32_t *dispenser, uint32_t n, Trac
       const bool can_step = busy && tr.lp >= tr.lend && !tr.finished();
       round = pending2 >= kRoundMin || __ballot_sync(0xffffffffu, can_step) == 0u;
     }
-    const bool stop = round && list_round<STACK, ANY>(tr, busy && tr.lp < tr.lend, any, cnt);
+    const bool stop = round && list_round<STACK, ANY, PER>(tr, busy && tr.lp < tr.lend, any, cnt);
     if (busy && (stop || tr.finished())) {
       done(ray, tr, any);
       ray = RayDispenser::kIdle;

@@ -109,7 +109,7 @@ __device__ __forceinline__ void warp_count(unsigned long long *p, unsigned long 
 // Persistent closest-hit kernel: warps take rays from the queue through a
 // RayDispenser (counters[4]) and interleave one octree entry per ray per
 // iteration, so finished lanes are refilled instead of idling.
-template <int STACK>
+template <int STACK, int PER>
 __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_closest(DevScene s, RayQ q, uint32_t *counters, uint32_t cur,
                                                        uint32_t *hit_ref, float *hit_t,
                                                        unsigned long long *stats, bool prof) {
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kTraceBlock, SNOG_TRACE_MINBLOCKS) k_trace_clo
     stats[0] += n;
   }
   TraceCounters c{0, 0, 0};
-  trace_loop<STACK, kClosestOnly>(
+  trace_loop<STACK, kClosestOnly, PER>(
       counters + 4, n, c,
       [&](uint32_t ray, Traversal<STACK> &tr, bool &any) {
         const float4 o = q.o[ray], d = q.d[ray];
@@ -560,7 +560,12 @@ void launch_bounce(const DevScene &s, const JobConsts &jc, WaveBuffers &wb, uint
   PathPtrs P{wb.thr, wb.rad, wb.pstate, wb.jit};
   const bool pf = prof != nullptr || count;
   if (prof) prof->begin(st, RenderProfile::CLOSEST);
-  k_trace_closest<STACK><<<resident_grid(k_trace_closest<STACK>, kTraceBlock), kTraceBlock, 0, st>>>(s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
+  if (s.pair_lists)
+    k_trace_closest<STACK, 2><<<resident_grid(k_trace_closest<STACK, 2>, kTraceBlock), kTraceBlock, 0, st>>>(
+        s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
+  else
+    k_trace_closest<STACK, 1><<<resident_grid(k_trace_closest<STACK, 1>, kTraceBlock), kTraceBlock, 0, st>>>(
+        s, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, wb.stats, pf);
   if (prof) prof->end(st), prof->begin(st, RenderProfile::SHADE);
   k_shade<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, cur, wb.hit_ref, wb.hit_t, P, qout, dl);
   k_direct<<<grid128, 128, 0, st>>>(s, jc, base, b, qin, wb.counters, wb.hit_ref, wb.hit_t, dl, sq);

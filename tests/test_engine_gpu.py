@@ -196,3 +196,19 @@ def test_direct_integrator_same_through_plain_batch_and_server():
     for img in (batch[0], served):
         assert np.allclose(img, plain, rtol=1e-5, atol=1e-6), np.abs(img - plain).max()
 
+
+
+def test_list_dealing_chosen_per_scene():
+    """The closest-hit traversal deals list entries in pairs for scenes whose
+    rays meet long lists (a random-triangle soup), one by one otherwise (the
+    terrain); either way a job's image is its plain render's."""
+    with sb.Scene(scenes.soup_scene(1_000_000, seed=25)) as soup, \
+            sb.Scene(scenes.terrain_scene(n=256, n_spheres=20, env_w=64, env_h=32)) as terrain:
+        assert soup.info()["pair_lists"] == 1
+        assert terrain.info()["pair_lists"] == 0
+        jobs = [(soup, scenes.orbit_camera(48, 40, np.random.default_rng(5)), sb.RenderParams(48, 40, 4, seed=3)),
+                (terrain, scenes.terrain_camera(40, 32), scenes.terrain_params(40, 32, 4, seed=4))]
+        imgs, _ = sb.render_batch(jobs)
+        for (sc, cam, p), img in zip(jobs, imgs):
+            ref, _ = sc.render(cam, p)
+            assert np.allclose(img, ref, rtol=1e-4, atol=1e-5), np.abs(img - ref).max()

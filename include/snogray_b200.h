@@ -249,7 +249,17 @@ int snog_ply_free(SnogPlyMesh *mesh);
  * scenes of 65536 surfaces or more. */
 enum { SNOG_OCTREE_AUTO = 0, SNOG_OCTREE_HOST = 1, SNOG_OCTREE_DEVICE = 2 };
 
-/* snog_scene_create with the octree builder chosen by OCTREE_MODE; replaces
+/* How the closest-hit traversal deals a node's surface list to the lanes of
+ * a warp, ORed into snog_scene_create_ex's OCTREE_MODE.  Hits, t values and
+ * traversal counts are the same in every mode; only the speed differs.
+ * PROBE (the default): pairs when random rays through the scene test more
+ * than 2.5 primitives per node visit (SnogSceneInfo::pair_lists); SINGLE:
+ * one entry per lane (up to 32 per round); PAIRED: two consecutive entries
+ * per lane (up to 64 per round). */
+enum { SNOG_LISTS_PROBE = 0, SNOG_LISTS_SINGLE = 1 << 8, SNOG_LISTS_PAIRED = 2 << 8 };
+
+/* snog_scene_create with the octree builder chosen by OCTREE_MODE (one
+ * SNOG_OCTREE_* value, optionally ORed with one SNOG_LISTS_* value); replaces
  * the same reference path (space/octree-builder.cc:173-650). */
 int snog_scene_create_ex(const SnogSceneDesc *desc, uint32_t octree_mode, SnogScene **out);
 

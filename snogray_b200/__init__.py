@@ -221,11 +221,17 @@ class Scene:
     once from the surfaces and lights, then rendered or traced."""
 
     OCTREE_AUTO, OCTREE_HOST, OCTREE_DEVICE = 0, 1, 2
+    LISTS = {"probe": 0, "single": 1 << 8, "paired": 2 << 8}   # SNOG_LISTS_*
 
-    def __init__(self, data: SceneData, device=True, octree=0):
+    def __init__(self, data: SceneData, device=True, octree=0, lists="probe"):
         """OCTREE picks the octree builder of a device scene (snog_scene_create_ex):
         OCTREE_AUTO, OCTREE_HOST or OCTREE_DEVICE; a host-only scene
-        (DEVICE=False) always uses the host builder."""
+        (DEVICE=False) always uses the host builder.  LISTS picks how the
+        closest-hit traversal deals node lists to lanes: "probe" (decided
+        from random rays at creation), "single" or "paired"; results are the
+        same in every mode."""
+        if lists not in self.LISTS:
+            raise ValueError(f"lists must be one of {sorted(self.LISTS)}")
         self.data = data
         keep = []
 
@@ -263,7 +269,7 @@ class Scene:
         d.mesh_right_handed = 1 if data.right_handed else 0
         h = _P()
         if device:
-            _check(_scene_create_ex(C.byref(d), octree, C.byref(h)))
+            _check(_scene_create_ex(C.byref(d), octree | self.LISTS[lists], C.byref(h)))
         else:
             _check(_scene_build_host(C.byref(d), C.byref(h)))
         self._h = h

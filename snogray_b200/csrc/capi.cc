@@ -302,7 +302,8 @@ int snog_scene_create(const SnogSceneDesc *desc, SnogScene **out) {
 int snog_scene_create_ex(const SnogSceneDesc *desc, uint32_t octree_mode, SnogScene **out) {
   return guarded([&] {
     if (!desc || !out) throw Error{SNOG_EINVAL, "null argument"};
-    if (octree_mode > SNOG_OCTREE_DEVICE) throw Error{SNOG_EINVAL, "unknown octree mode"};
+    if ((octree_mode & 0xffu) > SNOG_OCTREE_DEVICE || (octree_mode >> 8) > 2u)
+      throw Error{SNOG_EINVAL, "unknown octree mode"};
     *out = nullptr;
     SceneImpl *impl = build_scene(*desc, true, octree_mode);
     *out = new SnogScene{impl};

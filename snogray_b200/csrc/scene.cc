@@ -160,6 +160,9 @@ T *dev_upload(DeviceArena &a, const std::vector<T> &v) {
 
 SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode) {
   auto t_start = std::chrono::steady_clock::now();
+  // Bits 8-9: the SNOG_LISTS_* dealing; the low byte: the octree builder.
+  const uint32_t lists_mode = octree_mode & 0x300u;
+  octree_mode &= 0xffu;
   // ---- validation --------------------------------------------------------
   if (d.n_materials == 0 || !d.materials) fail("scene has no materials");
   for (uint32_t i = 0; i < d.n_materials; i++) {
@@ -544,7 +547,10 @@ SceneImpl *build_scene(const SnogSceneDesc &d, bool upload, uint32_t octree_mode
   D.horizon = horizon;
   D.max_depth = S.oct.max_depth;
   D.right_handed = d.mesh_right_handed ? 1u : 0u;
-  D.pair_lists = upload ? probe_pair_lists(D) : 0u;
+  D.pair_lists = !upload                             ? 0u
+                 : lists_mode == SNOG_LISTS_SINGLE ? 0u
+                 : lists_mode == SNOG_LISTS_PAIRED ? 1u
+                                                   : probe_pair_lists(D);
 
   SnogSceneInfo &I = S.info;
   std::memset(&I, 0, sizeof(I));

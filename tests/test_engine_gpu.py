@@ -198,6 +198,31 @@ def test_direct_integrator_same_through_plain_batch_and_server():
 
 
 
+def test_list_dealing_modes_give_identical_results():
+    """Dealing node lists one entry per lane and two per lane finds the same
+    hits in the same order: the same images bit for bit, on the plain
+    renderer and on the engine, and the same traversal counts, on a scene of
+    long lists (a random-triangle soup) and one of short lists (the terrain)."""
+    import dataclasses
+    cases = [(scenes.soup_scene(300_000, seed=25), scenes.orbit_camera(48, 40, np.random.default_rng(5)),
+              sb.RenderParams(48, 40, 4, seed=3)),
+             (scenes.terrain_scene(n=256, n_spheres=20, env_w=64, env_h=32), scenes.terrain_camera(40, 32),
+              scenes.terrain_params(40, 32, 4, seed=4))]
+    for sd, cam, p in cases:
+        with sb.Scene(sd, lists="single") as one, sb.Scene(sd, lists="paired") as two:
+            assert one.info()["pair_lists"] == 0 and two.info()["pair_lists"] == 1
+            counted = dataclasses.replace(p, flags=sb.SNOG_RENDER_COUNT_TRAVERSAL)
+            img1, st1 = one.render(cam, counted)
+            img2, st2 = two.render(cam, counted)
+            assert np.array_equal(img1, img2)
+            assert st1["closest_tests"] > 0
+            for k in ("closest_rays", "closest_nodes", "closest_tests", "shadow_nodes", "shadow_tests"):
+                assert st1[k] == st2[k], k
+            e1, _ = sb.render_batch([(one, cam, p)])
+            e2, _ = sb.render_batch([(two, cam, p)])
+            assert np.array_equal(e1[0], e2[0])
+
+
 def test_list_dealing_chosen_per_scene():
     """The closest-hit traversal deals list entries in pairs for scenes whose
     rays meet long lists (a random-triangle soup), one by one otherwise (the

@@ -83,6 +83,18 @@ def test_empty_scene_rejected():
         Scene(sd, device=False)
 
 
+@pytest.mark.parametrize("mode", [3, 3 << 8, 1 << 10, 0xff])
+def test_unknown_scene_modes_refused_before_any_device_work(mode):
+    """snog_scene_create_ex refuses an unknown octree builder or list
+    dealing (SNOG_LISTS_*) before it touches the device."""
+    import snogray_b200 as sb
+    with pytest.raises(sb.SnogError) as e:
+        Scene(scenes.cornell_box(), octree=mode)
+    assert e.value.code == sb.SNOG_EINVAL
+    with pytest.raises(ValueError):
+        Scene(scenes.cornell_box(), lists="triple")
+
+
 def test_glass_media_are_shared_and_bounded():
     """Glass materials with equal ior and absorption share one medium; more
     than 31 distinct media is refused (the path state's medium ids are 5

@@ -415,8 +415,9 @@ int snog_engine_autotune(SnogScene *const *scenes, const SnogCamera *cameras, co
       prm[k] = params[i];
       sample_paths += job_paths(prm[k]);
     }
-    // Aim for ~48M sample paths (several fills of the largest queue tried).
-    const double target = 48.0 * (1 << 20);
+    // Aim for ~128M sample paths: two fills of the largest queue tried, so
+    // each queue size is timed through its steady state and its drain.
+    const double target = 128.0 * (1 << 20);
     if (sample_paths > target) {
       const double f = target / double(sample_paths);
       sample_paths = 0;
@@ -470,7 +471,10 @@ int snog_engine_autotune(SnogScene *const *scenes, const SnogCamera *cameras, co
       }
       cur.*field = best_v;
     };
-    try_values(&EngineConfigHost::slots, {1u << 21, 1u << 22, 1u << 23, 1u << 24});
+    // Larger queues mean fewer, longer trace launches, each ending in one
+    // tail where SMs run out of rays (the 1920x1080 64-spp terrain frame:
+    // 16M slots 279.8 ms, 32M 273.6 ms, 64M 271.5 ms).
+    try_values(&EngineConfigHost::slots, {1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26});
     try_values(&EngineConfigHost::item_paths, {1u << 12, 1u << 14, 1u << 16, 1u << 18});
     try_values(&EngineConfigHost::iters_per_launch, {1u, 2u, 4u, 8u});
     to_abi(cur, best);

@@ -200,9 +200,12 @@ def test_direct_integrator_same_through_plain_batch_and_server():
 
 def test_list_dealing_modes_give_identical_results():
     """Dealing node lists one entry per lane and two per lane finds the same
-    hits in the same order: the same images bit for bit, on the plain
-    renderer and on the engine, and the same traversal counts, on a scene of
-    long lists (a random-triangle soup) and one of short lists (the terrain)."""
+    hits in the same order, on a scene of long lists (a random-triangle soup)
+    and one of short lists (the terrain): the same traversal counts, exactly
+    (a different hit would change the rest of its path), and the same images
+    on the plain renderer and the engine up to the order in which shadow
+    rays' contributions are added (float atomics: rtol 1e-4, the bar of the
+    engine-vs-plain tests)."""
     import dataclasses
     cases = [(scenes.soup_scene(300_000, seed=25), scenes.orbit_camera(48, 40, np.random.default_rng(5)),
               sb.RenderParams(48, 40, 4, seed=3)),
@@ -214,13 +217,13 @@ def test_list_dealing_modes_give_identical_results():
             counted = dataclasses.replace(p, flags=sb.SNOG_RENDER_COUNT_TRAVERSAL)
             img1, st1 = one.render(cam, counted)
             img2, st2 = two.render(cam, counted)
-            assert np.array_equal(img1, img2)
+            assert np.allclose(img1, img2, rtol=1e-4, atol=1e-5), np.abs(img1 - img2).max()
             assert st1["closest_tests"] > 0
             for k in ("closest_rays", "closest_nodes", "closest_tests", "shadow_nodes", "shadow_tests"):
                 assert st1[k] == st2[k], k
             e1, _ = sb.render_batch([(one, cam, p)])
             e2, _ = sb.render_batch([(two, cam, p)])
-            assert np.array_equal(e1[0], e2[0])
+            assert np.allclose(e1[0], e2[0], rtol=1e-4, atol=1e-5), np.abs(e1[0] - e2[0]).max()
 
 
 def test_list_dealing_chosen_per_scene():

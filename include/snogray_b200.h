@@ -296,6 +296,23 @@ int snog_trace(SnogScene *scene, const float *rays, uint32_t n, uint32_t n_close
 int snog_trace_device(SnogScene *scene, const float *d_rays, uint32_t n, uint32_t n_closest,
                       int32_t *d_prim, float *d_t, float *d_normal, void *stream);
 
+/* The path's shading functions at given sample parameters, for per-sample
+ * comparison with the reference's (material/bsdf.h:158-168,
+ * light/light-sampler.h): PROBES (HOST, 12 floats each: ray origin, t0 = 0,
+ * unit direction, t1, BSDF parameter u v, light parameter u v).  For each
+ * probe, the closest hit from the scene's default medium and there:
+ * Bsdf::sample at the BSDF parameter (all flags); for every light sampler,
+ * in the reference's order, its sample at the light parameter, Bsdf::eval
+ * at that sample's direction and the sampler's eval at the BSDF sample's
+ * direction.  EXTRA (HOST, may be NULL = 0.5): n x n_lights numbers for
+ * samplers that draw one more (the sphere light's, sphere-light-sampler.cc:90).
+ * OUT (HOST): n x (9 + 18 x n_lights) floats per probe: hit; BSDF sample val
+ * r g b, pdf, dir x y z (normal frame), flags; then per light: sample val
+ * r g b, pdf, dir x y z, dist, the extra number used; BSDF eval val r g b,
+ * pdf; light eval val r g b, pdf, dist.  Evaluations whose sample had pdf 0
+ * are left 0. */
+int snog_sample_probe(SnogScene *scene, const float *probes, const float *extra, uint32_t n, float *out);
+
 /* Render the whole image with the path integrator and the Mitchell-filtered
  * sampled output, into HOST memory out_rgb (height rows of width RGB floats,
  * top row first; the flushed values of ImageSampledOutput,

@@ -24,6 +24,14 @@
 //                                   a band of rows for a bounded CPU sample;
 //                                   with KEEP nonzero, repetition r writes
 //                                   OUT.pfm.r.pfm instead of overwriting OUT.pfm
+//   samples SPEC PROBES OUT         per probe (a ray and four parameters),
+//                                   Scene::intersect and make_intersect
+//                                   from the default medium, then the hit's
+//                                   Bsdf::sample / Bsdf::eval and every light
+//                                   sampler's sample / eval at the given
+//                                   parameters (render/intersect.h,
+//                                   material/bsdf.h:158-168,
+//                                   light/light-sampler.h)
 //
 // The reference keeps octree nodes, surface lists and camera fields private;
 // this program (and only this program) reads them by compiling the
@@ -84,6 +92,10 @@
 #include "render/global-render-state.h"
 #include "render/render-context.h"
 #include "render/render-stats.h"
+#include "render/intersect.h"
+#include "material/media.h"
+#include "material/bsdf.h"
+#include "light/light-sampler.h"
 #include "render-mgr/render-mgr.h"
 #include "render-mgr/render-pattern.h"
 #include "space/octree.h"
@@ -430,6 +442,85 @@ int mode_render(const std::string &spec, const std::string &out, unsigned thread
 
 // OUT: "OK" or "ERR" + message line; for OK then uint32 n_vertices,
 // n_normals, n_triangles and the float / uint32 arrays.
+// Probe file: uint32 n, then n x 12 floats (origin, t0, direction, t1,
+// BSDF parameter u v, light parameter u v).  Output: uint32 n, uint32
+// n_lights, then per probe kProbeOut floats: hit, BSDF sample (val[3], pdf,
+// dir[3] in the normal frame, flags), BSDF eval at the light sample's
+// direction (val[3], pdf, per light), light samples and evals -- the layout
+// below.  The sphere light sampler draws one extra number from the
+// context's generator (light/sphere-light-sampler.cc:90): the generator is
+// reseeded before each light's sample, and the number it will draw is
+// written out so a caller can feed the same value.
+constexpr int kProbeHead = 9;    // hit, bsdf sample val[3] pdf dir[3] flags
+constexpr int kProbeLight = 18;  // per light: sample val[3] pdf dir[3] dist extra;
+                                 // bsdf eval at it val[3] pdf; light eval at the
+                                 // bsdf sample's dir val[3] pdf
+
+int mode_samples(const std::string &spec, const std::string &probes_path, const std::string &out) {
+  RefScene rs;
+  build_scene(rs, spec);
+  std::ifstream in(probes_path, std::ios::binary);
+  uint32_t n = 0;
+  in.read(reinterpret_cast<char *>(&n), 4);
+  std::vector<float> pr(size_t(n) * 12);
+  in.read(reinterpret_cast<char *>(pr.data()), std::streamsize(pr.size() * 4));
+  if (!in) throw std::runtime_error("short probe file");
+  const Scene &scene = rs.grs->scene;
+  const uint32_t nl = scene.num_light_samplers();
+  const size_t stride = kProbeHead + size_t(kProbeLight) * nl;
+  std::vector<float> res(size_t(n) * stride, 0.f);
+  RenderContext ctx(*rs.grs);
+  for (uint32_t i = 0; i < n; i++) {
+    const float *q = &pr[size_t(i) * 12];
+    float *r = &res[size_t(i) * stride];
+    Ray ray(Pos(q[0], q[1], q[2]), Vec(q[4], q[5], q[6]), q[3], q[7]);
+    const Surface::Renderable::IsecInfo *ii = scene.intersect(ray, ctx);
+    if (!ii) continue;
+    Media media(ctx.default_medium);
+    Intersect isec = ii->make_intersect(media, ctx);
+    r[0] = 1.f;
+    const Bsdf *bsdf = isec.bsdf;
+    Bsdf::Sample bs;
+    if (bsdf) bs = bsdf->sample(UV(q[8], q[9]), Bsdf::ALL);
+    for (int c = 0; c < 3; c++) r[1 + c] = bs.val[c];
+    r[4] = bs.pdf;
+    r[5] = bs.dir.x; r[6] = bs.dir.y; r[7] = bs.dir.z;
+    r[8] = float(bs.flags);
+    for (uint32_t k = 0; k < nl; k++) {
+      float *l = r + kProbeHead + size_t(kProbeLight) * k;
+      const unsigned seed = 7919u * i + 104729u * k + 1u;
+      l[8] = Random(seed)();
+      ctx.random.seed(seed);
+      const Light::Sampler *ls = scene.light_samplers[k];
+      Light::Sampler::Sample s = ls->sample(isec, UV(q[10], q[11]));
+      for (int c = 0; c < 3; c++) l[c] = s.val[c];
+      l[3] = s.pdf;
+      l[4] = s.dir.x; l[5] = s.dir.y; l[6] = s.dir.z;
+      l[7] = float(s.dist);
+      if (bsdf && s.pdf != 0.f) {
+        Bsdf::Value bv = bsdf->eval(s.dir, Bsdf::ALL);
+        for (int c = 0; c < 3; c++) l[9 + c] = bv.val[c];
+        l[12] = bv.pdf;
+      }
+      if (bsdf && bs.pdf != 0.f) {
+        Light::Sampler::Value lv = ls->eval(isec, bs.dir);
+        for (int c = 0; c < 3; c++) l[13 + c] = lv.val[c];
+        l[16] = lv.pdf;
+        l[17] = float(lv.dist);
+      }
+    }
+    ctx.mempool.reset();
+  }
+  FILE *f = fopen(out.c_str(), "wb");
+  if (!f) throw std::runtime_error("cannot write " + out);
+  fwrite(&n, 4, 1, f);
+  fwrite(&nl, 4, 1, f);
+  fwrite(res.data(), 4, res.size(), f);
+  fclose(f);
+  printf("{\"probes\": %u, \"lights\": %u}\n", n, nl);
+  return 0;
+}
+
 int mode_ply(const char *file, const char *out_path) {
   Mesh mesh;
   Mesh::part_index_t part = mesh.add_part(new Lambert(Color(0.5f)));
@@ -475,6 +566,7 @@ int main(int argc, char **argv) {
     if (mode == "ply" && argc == 4) return mode_ply(argv[2], argv[3]);
     if (mode == "trace" && argc >= 5)
       return mode_trace(argv[2], argv[3], argv[4], argc > 5 ? atoi(argv[5]) : 1);
+    if (mode == "samples" && argc == 5) return mode_samples(argv[2], argv[3], argv[4]);
     if (mode == "render" && argc >= 4)
       return mode_render(argv[2], argv[3], argc > 4 ? atoi(argv[4]) : 1,
                          argc > 5 ? atoi(argv[5]) : 0, argc > 6 ? atoi(argv[6]) : 0,

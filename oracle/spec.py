@@ -253,3 +253,49 @@ def port_octree(scene, tmpdir=None):
         oc = read_octree(op)
     oc["stats"] = stats
     return oc
+
+
+PROBE_HEAD, PROBE_LIGHT = 9, 18     # oracle/ref_harness.cc kProbeHead, kProbeLight
+
+
+def camera_probes(camera, n, seed=0):
+    """N probes of SCENE's camera: rays through uniform random points of the
+    film (unit directions, extent [0, 1e30]) with uniform random BSDF and
+    light parameters.  Returns an (n, 12) float32 array in the layout the
+    harness's samples mode reads."""
+    rng = np.random.default_rng(seed)
+    fx = rng.uniform(-1, 1, n).astype(np.float32)
+    fy = rng.uniform(-1, 1, n).astype(np.float32)
+    fwd, right, up = (np.asarray(v, np.float64) for v in (camera.forward, camera.right, camera.up))
+    d = (fwd[None] + (fx * camera.tan_half_fov_x)[:, None] * right[None] +
+         (fy * camera.tan_half_fov_y)[:, None] * up[None])
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pr = np.zeros((n, 12), np.float32)
+    pr[:, 0:3] = np.asarray(camera.pos, np.float32)[None]
+    pr[:, 3] = 0.0
+    pr[:, 4:7] = d.astype(np.float32)
+    pr[:, 7] = 1e30
+    pr[:, 8:12] = rng.random((n, 4), np.float32)
+    return pr
+
+
+def read_samples(path):
+    """(n_lights, head (n, 9), lights (n, n_lights, 18)) from a samples file."""
+    raw = np.fromfile(path, np.uint8)
+    n, nl = raw[:8].view("<u4")
+    res = raw[8:].view("<f4").reshape(int(n), PROBE_HEAD + PROBE_LIGHT * int(nl))
+    return int(nl), res[:, :PROBE_HEAD].copy(), res[:, PROBE_HEAD:].reshape(int(n), int(nl), PROBE_LIGHT).copy()
+
+
+def ref_samples(scene, probes, flavour="parity", tmpdir=None):
+    """The reference's Bsdf::sample / eval and light samplers' sample / eval
+    at the probes' hits (harness mode `samples`)."""
+    probes = np.ascontiguousarray(probes, np.float32)
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, pp, op = (os.path.join(d, x) for x in ("s.spec", "p.bin", "o.bin"))
+        write_spec(sp, scene)
+        with open(pp, "wb") as f:
+            f.write(np.array([len(probes)], "<u4").tobytes())
+            f.write(probes.tobytes())
+        _run([ref_binary(flavour), "samples", sp, pp, op])
+        return read_samples(op)

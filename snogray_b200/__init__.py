@@ -147,6 +147,7 @@ _scene_info = _sig("snog_scene_info", C.c_int, _P, C.POINTER(SnogSceneInfo))
 _scene_octree = _sig("snog_scene_octree", C.c_int, _P, _P, _P, _P)
 _trace = _sig("snog_trace", C.c_int, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P)
 _trace_device = _sig("snog_trace_device", C.c_int, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P)
+_sample_probe = _sig("snog_sample_probe", C.c_int, _P, _P, _P, C.c_uint32, _P)
 _render = _sig("snog_render", C.c_int, _P, C.POINTER(SnogCamera), C.POINTER(SnogRenderParams), _P,
                C.POINTER(SnogRenderStats))
 _render_device = _sig("snog_render_device", C.c_int, _P, C.POINTER(SnogCamera),
@@ -325,6 +326,19 @@ class Scene:
         _check(_trace(self._h, _ptr(rays), n, n_closest, _ptr(prim), _ptr(t), _ptr(nrm), _ptr(cnt)))
         return prim, t, nrm, {"closest_nodes": int(cnt[0]), "closest_tests": int(cnt[1]),
                               "any_nodes": int(cnt[2]), "any_tests": int(cnt[3])}
+
+    def sample_probe(self, probes, extra=None):
+        """The shading functions at given parameters (snog_sample_probe):
+        PROBES is (n, 12) float32 (origin, t0 = 0, unit direction, t1, BSDF
+        u v, light u v); EXTRA is (n, n_lights) or None.  Returns (head
+        (n, 9), lights (n, n_lights, 18)) in the layout the header documents."""
+        pr = np.ascontiguousarray(probes, np.float32)
+        n = pr.shape[0]
+        nl = self.info()["n_lights"]
+        ex = None if extra is None else np.ascontiguousarray(extra, np.float32).reshape(n, nl)
+        out = np.zeros((n, 9 + 18 * nl), np.float32)
+        _check(_sample_probe(self._h, _ptr(pr), _ptr(ex), n, _ptr(out)))
+        return out[:, :9].copy(), out[:, 9:].reshape(n, nl, 18).copy()
 
     def trace_device(self, d_rays, n, n_closest, d_prim, d_t=None, d_normal=None, stream=None):
         """Device-pointer variant (integers, e.g. torch tensor .data_ptr())."""

@@ -107,6 +107,34 @@ TRACE_CASES = {
 }
 
 
+# Per-sample shading: probes through each camera's film (spec.camera_probes)
+# with random BSDF and light parameters, evaluated by the reference's
+# Bsdf::sample / eval and light samplers' sample / eval (harness mode
+# `samples`).  The scenes cover Lambert, Cook-Torrance, Mirror (conductor,
+# dielectric over Lambert, zero reflectance) and Glass materials, smooth
+# mesh normals, and tripar, sphere, point, spot, far and envmap lights.
+SAMPLE_CASES = {
+    "cornell": (scenes.cornell_box, lambda: scenes.cornell_camera(64, 64)),
+    "mirror": (scenes.mirror_scene, lambda: scenes.cornell_camera(64, 64)),
+    "spot_far": (scenes.spot_far_scene, lambda: scenes.spot_far_camera(64, 64)),
+    "terrain": (lambda: scenes.terrain_scene(n=96, n_spheres=40, seed=11, env_w=64, env_h=32),
+                lambda: scenes.terrain_camera(64, 48)),
+    "mesh_smooth": (lambda: scenes.mesh_scene(smooth=True), lambda: scenes.mesh_camera(48, 48)),
+    "nested_glass": (scenes.nested_glass_scene, lambda: scenes.cornell_camera(64, 64)),
+}
+SAMPLE_PROBES = 2048
+
+
+def gen_samples(name):
+    mk, cam = SAMPLE_CASES[name]
+    sd = mk()
+    probes = spec.camera_probes(cam(), SAMPLE_PROBES, seed=53)
+    nl, head, lights = spec.ref_samples(sd, probes)
+    np.savez_compressed(os.path.join(HERE, f"samples_{name}.npz"), probes=probes, head=head, lights=lights,
+                        n_lights=np.uint32(nl), scene_digest=scenes.scene_digest(sd))
+    print(f"samples_{name}: {int(head[:, 0].sum())} hits of {len(probes)}, {nl} lights")
+
+
 def gen_trace(name):
     make_scene, make_rays = TRACE_CASES[name]
     sd = make_scene()
@@ -225,7 +253,7 @@ def gen_terrain_full():
 if __name__ == "__main__":
     if not spec.have_ref():
         spec.build(["ref"])
-    which = sys.argv[1:] or ["trace", "render", "terrain_full"]
+    which = sys.argv[1:] or ["trace", "render", "terrain_full", "samples"]
     if "terrain_full" in which:
         gen_terrain_full()
     if "trace" in which:
@@ -234,6 +262,9 @@ if __name__ == "__main__":
     if "render" in which:
         for nm in RENDER_CASES:
             gen_render(nm)
+    if "samples" in which:
+        for nm in SAMPLE_CASES:
+            gen_samples(nm)
     for nm in which:
         if nm in RENDER_CASES:
             gen_render(nm)

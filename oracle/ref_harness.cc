@@ -24,6 +24,10 @@
 //                                   a band of rows for a bounded CPU sample;
 //                                   with KEEP nonzero, repetition r writes
 //                                   OUT.pfm.r.pfm instead of overwriting OUT.pfm
+//   filter IN OUT                   the image output's default filter,
+//                                   ImageMitchellFilt::val (x, y)
+//                                   (image/image-mitchell-filt.h:45-65), at
+//                                   IN's offsets (uint32 n, n x 2 floats)
 //   samples SPEC PROBES OUT         per probe (a ray and four parameters),
 //                                   Scene::intersect and make_intersect
 //                                   from the default medium, then the hit's
@@ -88,6 +92,7 @@
 #include "load/mesh/load-ply.h"
 #include "image/image.h"
 #include "image/image-sampled-output.h"
+#include "image/image-mitchell-filt.h"
 #include "camera/camera.h"
 #include "render/global-render-state.h"
 #include "render/render-context.h"
@@ -521,6 +526,24 @@ int mode_samples(const std::string &spec, const std::string &probes_path, const 
   return 0;
 }
 
+int mode_filter(const std::string &in_path, const std::string &out) {
+  std::ifstream in(in_path, std::ios::binary);
+  uint32_t n = 0;
+  in.read(reinterpret_cast<char *>(&n), 4);
+  std::vector<float> xy(size_t(n) * 2), v(n);
+  in.read(reinterpret_cast<char *>(xy.data()), std::streamsize(xy.size() * 4));
+  if (!in) throw std::runtime_error("short offsets file");
+  const ImageMitchellFilt filt;
+  for (uint32_t i = 0; i < n; i++) v[i] = filt.val(xy[2 * size_t(i)], xy[2 * size_t(i) + 1]);
+  FILE *f = fopen(out.c_str(), "wb");
+  if (!f) throw std::runtime_error("cannot write " + out);
+  fwrite(v.data(), 4, n, f);
+  fclose(f);
+  printf("{\"b\": %.9g, \"c\": %.9g, \"x_radius\": %.9g, \"y_radius\": %.9g}\n", filt.b, filt.c, filt.x_radius,
+         filt.y_radius);
+  return 0;
+}
+
 int mode_ply(const char *file, const char *out_path) {
   Mesh mesh;
   Mesh::part_index_t part = mesh.add_part(new Lambert(Color(0.5f)));
@@ -567,6 +590,7 @@ int main(int argc, char **argv) {
     if (mode == "trace" && argc >= 5)
       return mode_trace(argv[2], argv[3], argv[4], argc > 5 ? atoi(argv[5]) : 1);
     if (mode == "samples" && argc == 5) return mode_samples(argv[2], argv[3], argv[4]);
+    if (mode == "filter" && argc == 4) return mode_filter(argv[2], argv[3]);
     if (mode == "render" && argc >= 4)
       return mode_render(argv[2], argv[3], argc > 4 ? atoi(argv[4]) : 1,
                          argc > 5 ? atoi(argv[5]) : 0, argc > 6 ? atoi(argv[6]) : 0,

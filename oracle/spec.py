@@ -299,3 +299,16 @@ def ref_samples(scene, probes, flavour="parity", tmpdir=None):
             f.write(probes.tobytes())
         _run([ref_binary(flavour), "samples", sp, pp, op])
         return read_samples(op)
+
+
+def ref_filter(xy, flavour="parity", tmpdir=None):
+    """The reference's image filter, ImageMitchellFilt::val (x, y), at the
+    (n, 2) offsets XY.  Returns (values, info: b, c, radii)."""
+    xy = np.ascontiguousarray(xy, np.float32)
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        ip, op = os.path.join(d, "xy.bin"), os.path.join(d, "v.bin")
+        with open(ip, "wb") as f:
+            f.write(np.array([len(xy)], "<u4").tobytes())
+            f.write(xy.tobytes())
+        info = _run([ref_binary(flavour), "filter", ip, op])
+        return np.fromfile(op, "<f4").copy(), info

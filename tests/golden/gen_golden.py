@@ -125,6 +125,25 @@ SAMPLE_CASES = {
 SAMPLE_PROBES = 2048
 
 
+def filter_offsets():
+    """Offsets for the image filter: the knots (0, +-0.5, +-1, +-1.5, +-2 and
+    just inside and outside the radius) on both axes, plus uniform random
+    points over [-2.5, 2.5]^2."""
+    knots = np.array([0, 0.5, 1, 1.5, 2, 1.999, 2.001, 0.999, 1.001, 2.5], np.float32)
+    knots = np.concatenate([knots, -knots])
+    gx, gy = np.meshgrid(knots, knots)
+    rnd = np.random.default_rng(59).uniform(-2.5, 2.5, (4096, 2)).astype(np.float32)
+    return np.concatenate([np.stack([gx.ravel(), gy.ravel()], 1), rnd]).astype(np.float32)
+
+
+def gen_filter():
+    xy = filter_offsets()
+    v, info = spec.ref_filter(xy)
+    np.savez_compressed(os.path.join(HERE, "filter_mitchell.npz"), xy=xy, val=v,
+                        b=np.float32(info["b"]), c=np.float32(info["c"]), radius=np.float32(info["x_radius"]))
+    print(f"filter_mitchell: {len(xy)} offsets, b {info['b']}, c {info['c']}, radius {info['x_radius']}")
+
+
 def gen_samples(name):
     mk, cam = SAMPLE_CASES[name]
     sd = mk()
@@ -253,7 +272,7 @@ def gen_terrain_full():
 if __name__ == "__main__":
     if not spec.have_ref():
         spec.build(["ref"])
-    which = sys.argv[1:] or ["trace", "render", "terrain_full", "samples"]
+    which = sys.argv[1:] or ["trace", "render", "terrain_full", "samples", "filter"]
     if "terrain_full" in which:
         gen_terrain_full()
     if "trace" in which:
@@ -262,6 +281,8 @@ if __name__ == "__main__":
     if "render" in which:
         for nm in RENDER_CASES:
             gen_render(nm)
+    if "filter" in which:
+        gen_filter()
     if "samples" in which:
         for nm in SAMPLE_CASES:
             gen_samples(nm)

@@ -67,23 +67,6 @@ int guarded(F &&f) {
   }
 }
 
-// RAII device buffer for per-call temporaries.
-struct DevBuf {
-  void *p = nullptr;
-  explicit DevBuf(size_t n) {
-    if (n == 0) n = 16;
-    cudaError_t e = cudaMalloc(&p, n);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      throw Error{e == cudaErrorMemoryAllocation ? SNOG_ENOMEM : SNOG_ECUDA,
-                  std::string("cudaMalloc: ") + cudaGetErrorString(e)};
-    }
-  }
-  ~DevBuf() { cudaFree(p); }
-  template <class T>
-  T *as() const { return static_cast<T *>(p); }
-};
-
 void RenderCache::release() {
   wave_free(wb);
   cudaFree(accum);

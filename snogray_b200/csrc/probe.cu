@@ -86,20 +86,6 @@ __global__ void k_probe_shade(DevScene s, const float *__restrict__ pr, const fl
   }
 }
 
-// RAII device buffer.
-struct ProbeBuf {
-  void *p = nullptr;
-  explicit ProbeBuf(size_t bytes) {
-    if (bytes && cudaMalloc(&p, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      throw Error{SNOG_ENOMEM, "device allocation failed"};
-    }
-  }
-  ~ProbeBuf() { cudaFree(p); }
-  template <class T>
-  T *as() const { return static_cast<T *>(p); }
-};
-
 }  // namespace
 }  // namespace snog
 
@@ -126,7 +112,7 @@ extern "C" int snog_sample_probe(SnogScene *scene, const float *probes, const fl
       const float v[7] = {q[0], q[1], q[2], q[4], q[5], q[6], q[7]};
       for (int a = 0; a < 7; a++) soa[size_t(a) * n + i] = v[a];
     }
-    ProbeBuf d_soa(soa.size() * 4), d_pr(size_t(n) * 48), d_ex(extra ? size_t(n) * nl * 4 : 0),
+    DevBuf d_soa(soa.size() * 4), d_pr(size_t(n) * 48), d_ex(extra ? size_t(n) * nl * 4 : 0),
         d_prim(size_t(n) * 4), d_t(size_t(n) * 4), d_cnt(64), d_out(size_t(n) * stride * 4);
     check_cuda(cudaMemcpy(d_soa.p, soa.data(), soa.size() * 4, cudaMemcpyHostToDevice), "probe rays H2D");
     check_cuda(cudaMemcpy(d_pr.p, probes, size_t(n) * 48, cudaMemcpyHostToDevice), "probes H2D");

@@ -89,6 +89,26 @@ struct Error {
 
 void check_cuda(int err, const char *what);   // throws Error{SNOG_ECUDA}
 
+// RAII device buffer for per-call temporaries (at least 16 bytes, so a
+// zero-length request still yields a valid pointer).
+struct DevBuf {
+  void *p = nullptr;
+  explicit DevBuf(size_t n) {
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{e == cudaErrorMemoryAllocation ? SNOG_ENOMEM : SNOG_ECUDA,
+                  std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+    }
+  }
+  ~DevBuf() { cudaFree(p); }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  template <class T>
+  T *as() const { return static_cast<T *>(p); }
+};
+
 // Error flags the render kernels raise in their flag word: bit 0, a
 // traversal stack overflowed (a non-finite ray); bit 1, a path entered a
 // fifth nested medium (the path state holds four; the reference's media

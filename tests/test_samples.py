@@ -119,3 +119,19 @@ def test_device_shading_matches_reference_per_sample(name):
     assert m["hit_differs"] == 0 and m["flags_differ"] == 0, m
     for q in QUANTITIES:
         assert m[q][1] == 0, (q, m)
+
+
+def test_probe_refusals_before_device_work():
+    """snog_sample_probe refuses a host-only scene and null arguments with
+    SNOG_EINVAL before it touches the device."""
+    import ctypes
+
+    import snogray_b200 as sb
+    g = load("cornell")
+    with sb.Scene(scenes.cornell_box(), device=False) as sc:
+        with pytest.raises(sb.SnogError) as e:
+            sc.sample_probe(g["probes"][:4])
+        assert e.value.code == sb.SNOG_EINVAL and "host-only" in str(e.value)
+        out = np.zeros(64, np.float32)
+        assert sb._sample_probe(sc.handle, None, None, 4, out.ctypes.data_as(ctypes.c_void_p)) == sb.SNOG_EINVAL
+    assert sb._sample_probe(None, None, None, 0, None) == sb.SNOG_EINVAL

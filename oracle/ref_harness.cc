@@ -24,6 +24,9 @@
 //                                   a band of rows for a bounded CPU sample;
 //                                   with KEEP nonzero, repetition r writes
 //                                   OUT.pfm.r.pfm instead of overwriting OUT.pfm
+//   camera SPEC IN OUT              Camera::eye_ray directions of the
+//                                   spec's camera at IN's film locations
+//                                   (camera/camera.h:322-389)
 //   filter IN OUT                   the image output's default filter,
 //                                   ImageMitchellFilt::val (x, y)
 //                                   (image/image-mitchell-filt.h:45-65), at
@@ -382,6 +385,44 @@ int mode_trace(const std::string &spec, const std::string &rays_path, const std:
   return 0;
 }
 
+// The spec's pinhole camera, set field by field (camera/camera.h:322-389).
+Camera camera_of(const snogspec::SpecHeader &h) {
+  Camera camera;
+  camera.pos = Pos(h.cam_pos[0], h.cam_pos[1], h.cam_pos[2]);
+  camera.forward = Vec(h.cam_forward[0], h.cam_forward[1], h.cam_forward[2]);
+  camera.right = Vec(h.cam_right[0], h.cam_right[1], h.cam_right[2]);
+  camera.up = Vec(h.cam_up[0], h.cam_up[1], h.cam_up[2]);
+  camera.tan_half_fov_x = h.tan_half_fov_x;
+  camera.tan_half_fov_y = h.tan_half_fov_y;
+  return camera;
+}
+
+// Film locations (uint32 n, n x 2 floats u v) to Camera::eye_ray directions
+// (n x 3 floats; the direction is eye_vec, not normalised).
+int mode_camera(const std::string &spec, const std::string &in_path, const std::string &out) {
+  RefScene rs;
+  build_scene(rs, spec);
+  const Camera camera = camera_of(rs.spec.h);
+  std::ifstream in(in_path, std::ios::binary);
+  uint32_t n = 0;
+  in.read(reinterpret_cast<char *>(&n), 4);
+  std::vector<float> uv(size_t(n) * 2), d(size_t(n) * 3);
+  in.read(reinterpret_cast<char *>(uv.data()), std::streamsize(uv.size() * 4));
+  if (!in) throw std::runtime_error("short film-location file");
+  for (uint32_t i = 0; i < n; i++) {
+    const Ray r = camera.eye_ray(UV(uv[2 * size_t(i)], uv[2 * size_t(i) + 1]), 1.f);
+    d[3 * size_t(i)] = r.dir.x;
+    d[3 * size_t(i) + 1] = r.dir.y;
+    d[3 * size_t(i) + 2] = r.dir.z;
+  }
+  FILE *f = fopen(out.c_str(), "wb");
+  if (!f) throw std::runtime_error("cannot write " + out);
+  fwrite(d.data(), 4, d.size(), f);
+  fclose(f);
+  printf("{\"rays\": %u}\n", n);
+  return 0;
+}
+
 int mode_render(const std::string &spec, const std::string &out, unsigned threads,
                 unsigned seed_skip, unsigned spp_override, int row0, int rows, unsigned repeat,
                 bool keep) {
@@ -400,13 +441,7 @@ int mode_render(const std::string &spec, const std::string &out, unsigned thread
   // independent, reproducible stream for a single-threaded render.
   for (unsigned i = 0; i < seed_skip; i++) RenderContext skip(*rs.grs);
 
-  Camera camera;
-  camera.pos = Pos(h.cam_pos[0], h.cam_pos[1], h.cam_pos[2]);
-  camera.forward = Vec(h.cam_forward[0], h.cam_forward[1], h.cam_forward[2]);
-  camera.right = Vec(h.cam_right[0], h.cam_right[1], h.cam_right[2]);
-  camera.up = Vec(h.cam_up[0], h.cam_up[1], h.cam_up[2]);
-  camera.tan_half_fov_x = h.tan_half_fov_x;
-  camera.tan_half_fov_y = h.tan_half_fov_y;
+  Camera camera = camera_of(h);
 
   unsigned w = h.width, hgt = h.height;
   int y0 = 0, nrows = int(hgt);
@@ -591,6 +626,7 @@ int main(int argc, char **argv) {
       return mode_trace(argv[2], argv[3], argv[4], argc > 5 ? atoi(argv[5]) : 1);
     if (mode == "samples" && argc == 5) return mode_samples(argv[2], argv[3], argv[4]);
     if (mode == "filter" && argc == 4) return mode_filter(argv[2], argv[3]);
+    if (mode == "camera" && argc == 5) return mode_camera(argv[2], argv[3], argv[4]);
     if (mode == "render" && argc >= 4)
       return mode_render(argv[2], argv[3], argc > 4 ? atoi(argv[4]) : 1,
                          argc > 5 ? atoi(argv[5]) : 0, argc > 6 ? atoi(argv[6]) : 0,

@@ -312,3 +312,17 @@ def ref_filter(xy, flavour="parity", tmpdir=None):
             f.write(xy.tobytes())
         info = _run([ref_binary(flavour), "filter", ip, op])
         return np.fromfile(op, "<f4").copy(), info
+
+
+def ref_eye_dirs(scene, camera, u, v, flavour="parity", tmpdir=None):
+    """The reference's Camera::eye_ray directions (eye_vec, not normalised)
+    for CAMERA at film locations (U, V); returns an (n, 3) float32 array."""
+    uv = np.ascontiguousarray(np.stack([u, v], 1), np.float32)
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        sp, ip, op = (os.path.join(d, x) for x in ("s.spec", "uv.bin", "d.bin"))
+        write_spec(sp, scene, camera)
+        with open(ip, "wb") as f:
+            f.write(np.array([len(uv)], "<u4").tobytes())
+            f.write(uv.tobytes())
+        _run([ref_binary(flavour), "camera", sp, ip, op])
+        return np.fromfile(op, "<f4").reshape(-1, 3).copy()

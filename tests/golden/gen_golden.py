@@ -63,20 +63,35 @@ def edge_rays(sd, n_rand, seed):
     return np.concatenate(rays, axis=1)
 
 
-def camera_rays(cam, w, h, max_trace, seed):
-    """Eye rays as Camera::eye_ray makes them for jittered film positions
-    (camera/camera.cc:108-160): unnormalised direction, t1 = max_trace."""
+def camera_film_locs(w, h, seed):
+    """Film locations of one jittered sample per pixel, as
+    Renderer::render_packet forms them (render-mgr/renderer.cc:84):
+    u = x / width, v = (height - y) / height, in float32."""
     rng = np.random.default_rng(seed)
     n = w * h
     px = (np.arange(n) % w + rng.uniform(0, 1, n)).astype(np.float32)
     py = (np.arange(n) // w + rng.uniform(0, 1, n)).astype(np.float32)
     u = px / np.float32(w)
     v = (np.float32(h) - py) / np.float32(h)
+    return u, v
+
+
+def eye_dirs(cam, u, v):
+    """Camera::eye_vec (camera/camera.h:384-389) in float32, in the order the
+    camera kernels evaluate it: forward + right x tan_x + up y tan_y."""
     x = (np.float32(2) * u - np.float32(1)).astype(np.float32)
     y = (np.float32(2) * v - np.float32(1)).astype(np.float32)
     f, r, up = (np.asarray(a, np.float32) for a in (cam.forward, cam.right, cam.up))
-    d = (f[None] + (r[None] * x[:, None]) * np.float32(cam.tan_half_fov_x)
-         + (up[None] * y[:, None]) * np.float32(cam.tan_half_fov_y)).astype(np.float32)
+    return (f[None] + (r[None] * x[:, None]) * np.float32(cam.tan_half_fov_x)
+            + (up[None] * y[:, None]) * np.float32(cam.tan_half_fov_y)).astype(np.float32)
+
+
+def camera_rays(cam, w, h, max_trace, seed):
+    """Eye rays as Camera::eye_ray makes them for jittered film positions
+    (camera/camera.cc:108-160): unnormalised direction, t1 = max_trace."""
+    u, v = camera_film_locs(w, h, seed)
+    n = w * h
+    d = eye_dirs(cam, u, v)
     soa = np.empty((7, n), np.float32)
     soa[0:3] = np.asarray(cam.pos, np.float32)[:, None]
     soa[3:6] = d.T
@@ -134,6 +149,23 @@ def filter_offsets():
     gx, gy = np.meshgrid(knots, knots)
     rnd = np.random.default_rng(59).uniform(-2.5, 2.5, (4096, 2)).astype(np.float32)
     return np.concatenate([np.stack([gx.ravel(), gy.ravel()], 1), rnd]).astype(np.float32)
+
+
+# Cameras whose eye rays are pinned: (scene, camera, film width, height).
+CAMERA_CASES = {
+    "cornell": (scenes.cornell_box, lambda: scenes.cornell_camera(64, 64), 64, 64),
+    "terrain": (lambda: scenes.terrain_scene(n=96, n_spheres=40, seed=11, env_w=64, env_h=32),
+                lambda: scenes.terrain_camera(96, 54), 96, 54),
+}
+
+
+def gen_camera():
+    out = {}
+    for name, (mk, cam, w, h) in CAMERA_CASES.items():
+        u, v = camera_film_locs(w, h, seed=61)
+        out[name] = spec.ref_eye_dirs(mk(), cam(), u, v)
+    np.savez_compressed(os.path.join(HERE, "camera_eye_rays.npz"), **out)
+    print("camera_eye_rays:", {k: v.shape for k, v in out.items()})
 
 
 def gen_filter():
@@ -272,7 +304,7 @@ def gen_terrain_full():
 if __name__ == "__main__":
     if not spec.have_ref():
         spec.build(["ref"])
-    which = sys.argv[1:] or ["trace", "render", "terrain_full", "samples", "filter"]
+    which = sys.argv[1:] or ["trace", "render", "terrain_full", "samples", "filter", "camera"]
     if "terrain_full" in which:
         gen_terrain_full()
     if "trace" in which:
@@ -283,6 +315,8 @@ if __name__ == "__main__":
             gen_render(nm)
     if "filter" in which:
         gen_filter()
+    if "camera" in which:
+        gen_camera()
     if "samples" in which:
         for nm in SAMPLE_CASES:
             gen_samples(nm)
